@@ -1,0 +1,369 @@
+"""Benchmark of the LJ cell-list MD step on B200.
+
+Workload (default): 1,048,576-atom Lennard-Jones fcc system (64^3 x 4),
+density 0.8442, T* 0.72, rc 2.5, Gaussian isokinetic thermostat, FP32
+positions/velocities/forces with FP64 reductions, dt 0.005, cell list rebuilt
+every step.  Metric: atom-steps/s (N x steps / device seconds).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Timing: W untimed warm-up steps, then K timed steps in CUDA-graph units of 2
+steps, each unit bracketed by CUDA events on the handle's stream with the L2
+flushed (a 256 MB write) before it; value = N * K / sum of unit times, max over
+ranks.  With --gpus N > 1 (torchrun) every rank runs its own replica of the
+system (the path does not shard across GPUs: replicas only, weak scaling).
+
+`e2e` runs the reference driver loop through the public API with host
+buffers: import from host memory, then per step one pb_md_run call and a
+temperature read-back (as testMD2.cu:149-168 does), then the final positions
+copied back; wall-clock time.  `cpu_baseline` is the FP64 oracle (OpenMP,
+all host cores) on a bounded sample of the same system.  `--impl reference`
+times the reference's own MD kernels compiled for the CPU (oracle/_ref), or the
+oracle port where that build is absent.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DT = 0.005
+METRIC = "LJ atom-steps/s at 1M atoms (Gaussian NVT, cell list rebuilt every step)"
+UNIT = "atom-steps/s"
+WORKLOAD = "lj_fcc_1048576_gauss_rho0.8442_T0.72_rc2.5"
+
+
+# --------------------------------------------------------------------------- utils
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Dist:
+    """torch.distributed plumbing: barrier and max/sum over ranks."""
+
+    def __init__(self, use_cuda: bool):
+        self.ws, self.rank, self.local = dist_env()
+        self.pg = None
+        if self.ws > 1:
+            import datetime
+            import torch
+            import torch.distributed as td
+            backend = "nccl" if use_cuda else "gloo"
+            td.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+            self.td, self.torch = td, torch
+            self.dev = torch.device("cuda", self.local) if use_cuda else torch.device("cpu")
+
+    def barrier(self):
+        if self.ws > 1:
+            self.td.barrier()
+
+    def reduce(self, x: float, op: str) -> float:
+        if self.ws == 1:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.dev)
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX if op == "max" else self.td.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.ws > 1:
+            self.td.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx.append(float(f[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh)
+    except Exception:
+        return {}
+
+
+def profiled_traffic(name: str):
+    """DRAM bytes per launch recorded from an ncu capture (profiles/*.txt)."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    try:
+        for line in open(path):
+            k, _, v = line.partition(":")
+            if k.strip() == name:
+                return float(v.split()[0])
+    except Exception:
+        pass
+    return None
+
+
+# --------------------------------------------------------------------------- CPU arms
+
+def run_cpu_oracle(steps: int) -> dict:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    from particlebase_b200 import workloads as W
+    po.build(ref=True)
+    s = W.config_c2()
+    O = po.Oracle(s.box, s.lj, s.rc, s.r, s.v)
+    O.run(1, DT, mode="gauss")  # warm
+    t = time.perf_counter()
+    O.run(steps, DT, mode="gauss")
+    el = time.perf_counter() - t
+    return {"value": s.n * steps / el, "unit": UNIT, "cores": po.lib().orc_threads(),
+            "kind": "port",
+            "sample": f"{steps} Gaussian steps of the full 1,048,576-atom system, FP64 oracle "
+                      f"(oracle/oracle.cpp), OpenMP", "seconds": el}
+
+
+def run_reference_arm(args) -> dict:
+    """The reference's own kernels on the host cores (oracle/_ref)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    from particlebase_b200 import workloads as W
+    try:
+        po.build(ref=True)
+    except Exception:
+        pass
+    s = W.config_c2()
+    steps = max(1, min(args.steps, 8))
+    if po.ref_available():
+        R = po.RefKernels(s.box, s.rc, s.r, s.v, s.mass, s.types, [1.0, 1.0], gaussian=True)
+        for _ in range(max(1, min(args.warmup, 2))):
+            R.run(DT, 1)  # includes the first (from-scratch) sort
+        t = time.perf_counter()
+        rc = R.run(DT, steps)
+        el = time.perf_counter() - t
+        kind, cores = "reference", po.ref().ref_threads()
+        sample = (f"{steps} steps of the full 1,048,576-atom Gaussian system: the reference's "
+                  f"kernels (kernelfuncs.cu, kerneltemplate.hh) compiled for the CPU, "
+                  f"one-thread blocks run in parallel by OpenMP; NR rc={rc}")
+    else:
+        O = po.Oracle(s.box, s.lj, s.rc, s.r, s.v)
+        O.run(1, DT, mode="gauss")
+        t = time.perf_counter()
+        O.run(steps, DT, mode="gauss")
+        el = time.perf_counter() - t
+        kind, cores = "port", po.lib().orc_threads()
+        sample = f"{steps} Gaussian steps of the full system, FP64 oracle port"
+    v = s.n * steps / el
+    return {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": 0,
+            "steps": steps, "warmup": args.warmup, "higher_is_better": True,
+            "config": {"workload": WORKLOAD, "atoms": s.n, "dt": DT},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# --------------------------------------------------------------------------- GPU arm
+
+def flush_l2(buf):
+    buf.zero_()
+
+
+def run_ours(args, dist: Dist) -> dict:
+    import torch
+    torch.cuda.set_device(dist.local)
+    from particlebase_b200 import workloads as W
+    from particlebase_b200.md import from_system
+    from particlebase_b200 import _lib as L
+
+    s = W.config_c2(seed=2 + dist.rank)
+    p = from_system(s, gaussian=True, fp64_velocities=False)
+    p.clearForce()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+
+    # warm-up (W steps, rounded up to whole graph units)
+    p.run(DT, max(2, args.warmup + (args.warmup % 2)))
+    torch.cuda.synchronize()
+
+    steps = args.steps + (args.steps % 2)
+    dist.barrier()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        t_ms = 0.0
+        for _ in range(steps // 2):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            t_ms += p.run_timed(DT, 2)
+        torch.cuda.synchronize()
+        warm_ms = p.run_timed(DT, steps)
+    dist.barrier()
+    clocks = clk.summary()
+    status = p.status()
+    t_max = dist.reduce(t_ms, "max") / 1e3
+    value = dist.ws * s.n * steps / t_max
+    warm_value = s.n * steps / (warm_ms / 1e3)
+
+    # phase breakdown and the force kernel's roofline
+    prof = p.profile(DT, 6)
+    p.calcBlockID()
+    p.calcForce(energy=True)
+    ps = p.pair_stats()
+    flops = 8.0 * ps["ncand"] + 14.0 * ps["nin"]
+    rc_peak = C_double = None
+    import ctypes as C
+    pk = C.c_double()
+    L.check(L.lib().pb_peak_fp32(C.byref(pk)), "peak_fp32")
+    fp32_peak = pk.value
+    force_s = prof["force"] / 1e3
+    achieved = flops / force_s / 1e12
+    C_cells = p.grid()[2]
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    cells_bytes = 36.0 * s.n + 8.0 * C_cells
+    evolve_bytes = 60.0 * s.n
+    traffic = profiled_traffic("k_force")
+
+    # e2e through the public API with host buffers (reference driver loop)
+    e2e_steps = max(4, min(steps, 50))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    q = from_system(s, gaussian=True, fp64_velocities=False)
+    q.clearForce()
+    temps = []
+    for _ in range(e2e_steps):
+        q.run(DT, 1)
+        temps.append(q.calcTemp())
+    r_final = q.getPosition()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_value = dist.ws * s.n * e2e_steps / dist.reduce(e2e_s, "max")
+    h2d = s.n * (16 + 16 + 4 + 4 + 2)
+    d2h = 8 * e2e_steps + r_final.nbytes
+    q.close()
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.ws, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": t_max * 1e3 / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 reductions)",
+        "data": "synthetic fcc lattice + Maxwell-Boltzmann velocities (seeded)",
+        "config": {"workload": WORKLOAD, "atoms_per_gpu": s.n, "cells": C_cells,
+                   "grid": [int(x) for x in p.grid()[0]], "dt": DT, "thermostat": "gaussian",
+                   "parallelism": f"replicas x{dist.ws}" if dist.ws > 1 else "single",
+                   "l2": "flushed (256 MB write) before every timed 2-step graph unit"},
+        "warm_l2_value": warm_value,
+        "phase_ms": prof,
+        "roofline": {"kernel": "k_force", "bound": "fp32", "achieved": achieved,
+                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                     "peak_source": "measured FFMA loop (pb_peak_fp32), FP32 non-tensor",
+                     "flops_per_atom_step": flops / s.n,
+                     "ncand_per_atom": ps["ncand"] / s.n, "nin_per_atom": ps["nin"] / s.n,
+                     "traffic": traffic},
+        "hbm_kernels": {
+            "cell_build": {"alg_bytes": cells_bytes, "ms": prof["cells"],
+                           "achieved_gbs": cells_bytes / (prof["cells"] / 1e3) / 1e9,
+                           "peak_gbs": hbm, "frac": (cells_bytes / (prof["cells"] / 1e3) / 1e9 / hbm)
+                           if hbm else None},
+            "evolve": {"alg_bytes": evolve_bytes, "ms": prof["evolve"],
+                       "achieved_gbs": evolve_bytes / (prof["evolve"] / 1e3) / 1e9,
+                       "peak_gbs": hbm, "frac": (evolve_bytes / (prof["evolve"] / 1e3) / 1e9 / hbm)
+                       if hbm else None}},
+        "clocks": clocks,
+        "device_status": status,
+        "gpu_launches": 9 * steps,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
+                "d2h_bytes_per_step": d2h / e2e_steps, "steps": e2e_steps,
+                "includes": "import from host, per-step pb_md_run + temperature read-back, "
+                            "final positions to host"},
+    }
+    p.close()
+    return out
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    args.warmup = max(3, args.warmup)
+
+    ws, rank, _ = dist_env()
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference_arm(args)), flush=True)
+        return 0
+
+    dist = Dist(use_cuda=True)
+    try:
+        out = run_ours(args, dist)
+        if dist.rank == 0:
+            if dist.ws == 1 and not args.no_cpu_baseline:
+                out["cpu_baseline"] = run_cpu_oracle(args.cpu_steps)
+            print(json.dumps(out), flush=True)
+    finally:
+        dist.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

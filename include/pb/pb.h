@@ -1,0 +1,213 @@
+/*
+ * particlebase_b200 — C ABI of the B200-native Lennard-Jones cell-list step.
+ *
+ * One pb_md handle is one periodic MD system resident on the current CUDA
+ * device: the state the reference keeps in a cudaParticleMD / cudaParticleVV /
+ * GaussianThermo object (cudaParticleBase.hh:29-226, cudaCutoffBlock.hh:28-133,
+ * cudaSortedPositions.hh:6-36, cudaParticleMD.hh:32-194, GaussianThermo.hh:14-90).
+ * The C++ classes in particlebase_b200/shim/ (same names and methods as the
+ * reference) are a thin layer over these functions, so the reference's
+ * testMD drivers compile against them unchanged.
+ *
+ * Conventions
+ *  - Every function returns pb_status (0 = success) and never calls exit();
+ *    pb_md_last_error() describes the last failure of a handle.
+ *  - Plain pointers and sizes only.  Host arrays are read or written
+ *    synchronously with respect to the handle's stream.
+ *  - All device work of a handle is issued on its stream (default: a stream
+ *    the handle creates); pb_md_set_stream() selects another one.
+ *  - Positions, velocities and forces use the reference's layouts: float4
+ *    per particle (x, y, z, w) in particle order; FP64 velocities of the
+ *    Gaussian thermostat as three planes x[N], y[N], z[N].
+ */
+#ifndef PB_PB_H
+#define PB_PB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pb_status {
+  PB_OK = 0,
+  PB_ERR_ARG = 1,          /* invalid argument or size */
+  PB_ERR_CUDA = 2,         /* a CUDA call failed */
+  PB_ERR_STATE = 3,        /* call out of order (e.g. force before cells) */
+  PB_ERR_NOCONVERGE = 4,   /* thermostat solve failed (reference: exit(0)) */
+  PB_ERR_UNSUPPORTED = 5,  /* feature outside this build (e.g. open boundaries) */
+  PB_ERR_OOM = 6,          /* device allocation or HBM budget exceeded */
+  PB_ERR_DEVICE = 7,       /* a kernel reported a status bit (see pb_md_status) */
+  PB_ERR_NOTFOUND = 8      /* unknown job / field */
+} pb_status;
+
+/* Host particle record, binary-compatible with the reference's ParticleBase
+ * (ParticleBase.hh:10-18): double r[3], m, v[3]; bool isFixed; double a[3];
+ * uint32_t type. */
+typedef struct pb_particle {
+  double r[3];
+  double m;
+  double v[3];
+  uint8_t is_fixed;
+  double a[3];
+  uint32_t type;
+} pb_particle;
+
+typedef struct pb_md pb_md;
+
+/* Creation flags */
+#define PB_MD_VEL_FP64 0x1u   /* keep velocities in FP64 planes (GaussianThermo::vd) */
+#define PB_MD_ACC_FP64 0x2u   /* accumulate per-atom force sums in FP64 */
+
+/* Fields for pb_md_get / pb_md_set */
+typedef enum pb_field {
+  PB_FIELD_R = 0,          /* float4[N]   positions                       (get/set) */
+  PB_FIELD_V = 1,          /* float4[N]   velocities (FP32 path)          (get/set) */
+  PB_FIELD_VD = 2,         /* double[3N]  velocities, FP64 planes         (get/set) */
+  PB_FIELD_F = 3,          /* float4[N]   force F(t)                      (get/set) */
+  PB_FIELD_FOLD = 4,       /* float4[N]   previous force (VV Fold)        (get/set) */
+  PB_FIELD_MINV = 5,       /* float[N]    1/mass                          (get/set) */
+  PB_FIELD_TYPE = 6,       /* uint16[N]   type id                         (get/set) */
+  PB_FIELD_CELL_OF = 7,    /* uint32[N]   reference cell id of each atom  (get) */
+  PB_FIELD_PID = 8,        /* uint32[N]   particle id per sorted slot     (get) */
+  PB_FIELD_CELL_START = 9, /* uint32[C+1] first slot of each cell, in key order (get) */
+  PB_FIELD_CELL_KEY = 10,  /* uint32[C]   key of each reference cell id   (get) */
+  PB_FIELD_NEIGHBORS = 11, /* uint32[27C] 27-neighbour table, reference order (get) */
+  PB_FIELD_R_SORTED = 12,  /* float4[N]   sorted positions, w = type bits (get) */
+  PB_FIELD_MASS = 13       /* float[N]    mass                            (get) */
+} pb_field;
+
+/* Energy / reduction results of pb_md_reduce */
+typedef struct pb_md_sums {
+  double mv2;       /* sum m v^2 (3 N kB T) */
+  double fv;        /* sum F . v */
+  double pe;        /* potential energy, truncated and unshifted, sum_{i<j} */
+  double pe_shift;  /* potential energy shifted by U(rc) per pair (conserved with KE) */
+  double virial;    /* sum_{i<j} r_ij . f_ij */
+  double xi;        /* Gaussian thermostat friction of the last step */
+} pb_md_sums;
+
+/* ---- lifetime ------------------------------------------------------------ */
+
+/* cudaParticleBase::setup + cudaParticleVV::setup + cudaParticleMD::setup +
+ * GaussianThermo::setup (cudaParticleBase.cu:18-66, cudaParticleVV.cu:5-8,
+ * cudaParticleMD.cu:13-22, GaussianThermo.cu:9-14). */
+int pb_md_create(uint32_t n, uint32_t flags, pb_md **out);
+/* The destructors (cudaParticleBase.cu:7-16 and siblings). */
+int pb_md_destroy(pb_md *h);
+/* Issue all work of the handle on `stream` (a cudaStream_t). */
+int pb_md_set_stream(pb_md *h, void *stream);
+const char *pb_md_last_error(const pb_md *h);
+/* Device status bits raised by kernels since the last call (cleared on read). */
+int pb_md_status(pb_md *h, uint32_t *bits);
+
+/* ---- set-up ---------------------------------------------------------------- */
+
+/* cudaFrame::setCell (cudaFrame.cu:85-91): xmin, xmax, ymin, ymax, zmin, zmax. */
+int pb_md_set_cell(pb_md *h, const float cell6[6]);
+/* cudaParticleMD::setLJparams -> _setLJparams (cudaParticleMD.cu:200-202,
+ * kernelinline.hh:120-134): (sigma, epsilon) per ordered type pair,
+ * ntypes <= 8.  The cutoff is the global rmax2 (pb_md_set_rmax2). */
+int pb_md_set_lj(pb_md *h, const float *sigma_eps, uint32_t ntypes);
+/* Extension: (sigma, epsilon, rc) per type pair; per-pair cutoffs. */
+int pb_md_set_lj_cut(pb_md *h, const float *sigma_eps_rc, uint32_t ntypes);
+/* Public field cudaParticleMD::rmax2 (cudaParticleMD.hh:160). */
+int pb_md_set_rmax2(pb_md *h, float rmax2);
+/* Public field cudaParticleMD::kB (cudaParticleMD.hh:94). */
+int pb_md_set_kB(pb_md *h, float kB);
+/* cudaParticleMD::import (cudaParticleMD.cu:327-336 -> cudaParticleBase.cu:68-117,
+ * GaussianThermo.cu:16-28) followed by setM (cudaParticleMD.cu:135-138). */
+int pb_md_import(pb_md *h, const pb_particle *p, uint32_t n);
+/* Same, from structure-of-arrays host buffers (r3, v3: 3 doubles per atom). */
+int pb_md_import_arrays(pb_md *h, const double *r3, const double *v3, const double *mass,
+                        const uint32_t *type);
+/* cudaParticleMD::setupCutoffBlock -> cudaCutoffBlock::setupCutoffBlock +
+ * setupSortedPositions (cudaParticleMD.hh:71-74, cudaCutoffBlock.cu:75-231).
+ * Only periodic boxes are supported (periodic = 0 -> PB_ERR_UNSUPPORTED). */
+int pb_md_setup_cells(pb_md *h, float rmax, int periodic);
+/* Grid of the last setup: cells per axis and cell edge (blocknum, blocklen). */
+int pb_md_grid(const pb_md *h, uint32_t n3[3], float len3[3], uint32_t *ncells);
+
+/* ---- the step ------------------------------------------------------------- */
+
+/* cudaParticleMD::calcBlockID (cudaParticleMD.hh:64-67 ->
+ * cudaCutoffBlock.cu:233-258, cudaSortedPositions.cu:27-30). */
+int pb_md_build_cells(pb_md *h);
+/* cudaParticleMD::calcForce (cudaParticleMD.cu:24-69).  flags: PB_FORCE_ENERGY
+ * also accumulates PE, shifted PE and virial (FP64) for pb_md_reduce. */
+#define PB_FORCE_ENERGY 0x1u
+int pb_md_force(pb_md *h, uint32_t flags);
+/* cudaParticleVV::clearForce (cudaParticleVV.cu:10-15): F = Fold = 0. */
+int pb_md_clear_force(pb_md *h);
+/* cudaParticleVV::TimeEvolution (cudaParticleVV.cu:17-34). */
+int pb_md_step_vv(pb_md *h, float dt);
+/* GaussianThermo::TimeEvolution (GaussianThermo.cu:29-77), solved on the
+ * device in closed form; tol is accepted for interface parity. */
+int pb_md_step_gauss(pb_md *h, float dt, double tol);
+/* cudaParticleBase::treatPeriodicCondition (cudaParticleBase.cu:175-184). */
+int pb_md_wrap(pb_md *h);
+/* Whole steps in the reference driver order (testMD2.cu:149-168 without the
+ * temperature policy): build cells, force, time evolution with the wrap
+ * fused.  mode 0: velocity Verlet, 1: Gaussian.  Captured as a CUDA graph
+ * after the first call with the same (dt, mode). */
+#define PB_MODE_VV 0
+#define PB_MODE_GAUSS 1
+int pb_md_run(pb_md *h, float dt, int mode, uint32_t steps);
+/* pb_md_run bracketed by CUDA events on the handle's stream; *ms = elapsed. */
+int pb_md_run_timed(pb_md *h, float dt, int mode, uint32_t steps, float *ms);
+
+/* Per-phase device time of `steps` eager steps, measured with CUDA events on
+ * the handle's stream: ms[0] cell build, ms[1] force, ms[2] time evolution
+ * (averages per step). */
+int pb_md_profile(pb_md *h, float dt, int mode, uint32_t steps, double ms[3]);
+/* Pair statistics of the current cell list: out[0] = ordered candidate pairs
+ * over the 27-cell stencil (i != j), out[1] = ordered pairs inside the cutoff
+ * counted by the last pb_md_force with PB_FORCE_ENERGY. */
+int pb_md_pair_stats(pb_md *h, double out[2]);
+
+/* ---- reductions and velocity control -------------------------------------- */
+
+/* Sums of the current state: calcMV2 (cudaParticleMD.cu:124-133,
+ * GaussianThermo.cu:79-87) in FP64, sum F.v (constTemp, cudaParticleMD.cu:140-155),
+ * and PE / virial of the last force call with PB_FORCE_ENERGY. */
+int pb_md_reduce(pb_md *h, pb_md_sums *out);
+/* cudaParticleMD::calcTemp (cudaParticleMD.hh:89-92): sum m v^2 / (3 N kB). */
+int pb_md_temperature(pb_md *h, double *T);
+/* scaleTemp (cudaParticleMD.cu:168-175, GaussianThermo.cu:89-96): v *= s. */
+int pb_md_scale_velocities(pb_md *h, double s);
+/* adjustVelocities (cudaParticleMD.cu:177-198, GaussianThermo.cu:98-119):
+ * zero mean per axis, standard deviation v1 per axis. */
+int pb_md_adjust_velocities(pb_md *h, double v1);
+/* Mean particle mass m0 of the last import (cudaParticleMD.cu:327-336). */
+int pb_md_mean_mass(const pb_md *h, double *m0);
+
+/* ---- state access ----------------------------------------------------------- */
+
+/* getPosition / getForce / getTypeID (cudaParticleBase.cu:119-149) and the
+ * other arrays listed in pb_field; `bytes` must equal the field size. */
+int pb_md_get(pb_md *h, int field, void *host, size_t bytes);
+int pb_md_set(pb_md *h, int field, const void *host, size_t bytes);
+int pb_md_field_bytes(const pb_md *h, int field, size_t *bytes);
+int pb_md_size(const pb_md *h, uint32_t *n);
+
+/* Host-only (no device work): the cell grid setupCutoffBlock would build for
+ * this box and cutoff -- blocknum = (uint32)(L / rmax), blocklen = L / blocknum
+ * in FP32 (cudaCutoffBlock.cu:97-101).  Returns PB_ERR_ARG if an axis would
+ * have fewer than 3 cells. */
+int pb_plan_grid(const float cell6[6], float rmax, uint32_t n3[3], float len3[3]);
+/* Host-only: Z-order rank of every (x, y) column, rank[d0 * ny + d1]. */
+int pb_plan_columns(uint32_t nx, uint32_t ny, uint32_t *rank);
+
+/* Measured FP32 FMA throughput of the current device (TFLOP/s), from a
+ * register-resident FFMA loop timed with CUDA events. */
+int pb_peak_fp32(double *tflops);
+
+/* Library version string. */
+const char *pb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PB_PB_H */

@@ -1,0 +1,191 @@
+// Cell-list build: bin every atom into its cell, counting-sort the atoms by
+// packed cell key, and gather sorted positions.
+//
+// Replaces cudaCutoffBlock::calcBlockID + cudaSortedPositions::calcBlockID
+// (cudaCutoffBlock.cu:233-258, cudaSortedPositions.cu:27-30), i.e. calcBID_F4,
+// sortByBID_M1, the single-CTA sortByBID, makeBindex and copyWithIndex
+// (kernelfuncs.cu:807-932).  The cell of each atom is computed with the same
+// FP32 arithmetic as calcBID_F4, so cell membership is bit-identical; the
+// within-cell order is canonical (ascending particle id) instead of the
+// reference's history-dependent order.
+//
+// Kernels, in launch order:
+//   k_bin       read r (16 B/atom), write key + within-cell ticket (8 B/atom)
+//   k_scan_*    exclusive scan of per-cell counts -> start[], zero the counts
+//   k_scatter   pid_tmp[start[key] + ticket] = i
+//   k_canon     one warp per cell: order members by particle id, write pid,
+//               slot and the sorted position float4 (type id in .w)
+#include "md.cuh"
+
+namespace pb {
+namespace {
+
+constexpr int kScanTile = 4096;  // counts per scan tile (1024 threads x 4)
+
+__device__ __forceinline__ uint32_t system_of(const CellBufs &b, uint32_t i) {
+  return b.sysid ? b.sysid[i] : 0u;
+}
+
+__global__ void __launch_bounds__(256) k_bin(CellBufs b) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= b.N) return;
+  const SysDesc &S = b.sys[system_of(b, i)];
+  const float4 p = b.r[i];
+  const int d0 = cell_coord(p.x, S.g.lo[0], S.g.len[0], S.g.n[0]);
+  const int d1 = cell_coord(p.y, S.g.lo[1], S.g.len[1], S.g.n[1]);
+  const int d2 = cell_coord(p.z, S.g.lo[2], S.g.len[2], S.g.n[2]);
+  const uint32_t rank = b.colrank[S.col0 + d0 * S.g.n[1] + d1];
+  const uint32_t key = S.cell0 + rank * (uint32_t)S.g.n[2] + (uint32_t)d2;
+  b.key[i] = key;
+  b.within[i] = atomicAdd(&b.count[key], 1u);
+}
+
+// Tile-local exclusive scan of kScanTile counts; writes the tile total and
+// zeroes the counts for the next build.
+__global__ void __launch_bounds__(1024) k_scan_tiles(CellBufs b) {
+  __shared__ uint32_t warp_tot[32];
+  const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * 4;
+  uint32_t c[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const uint32_t idx = base + k;
+    c[k] = idx < b.ncells ? b.count[idx] : 0u;
+  }
+  uint32_t sum = c[0] + c[1] + c[2] + c[3];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = warp_tot[lane];
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    warp_tot[lane] = wi - w;  // exclusive prefix of warp totals
+    if (lane == 31) b.tilesum[blockIdx.x] = wi;
+  }
+  __syncthreads();
+  uint32_t run = warp_tot[warp] + incl - sum;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const uint32_t idx = base + k;
+    if (idx < b.ncells) {
+      b.start[idx] = run;
+      b.count[idx] = 0u;
+    }
+    run += c[k];
+  }
+}
+
+// Exclusive scan of the tile totals (single block; up to 1024 * 32 tiles).
+__global__ void __launch_bounds__(1024) k_scan_top(CellBufs b, uint32_t ntiles) {
+  __shared__ uint32_t warp_tot[32];
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint32_t base = 0; base < ntiles; base += blockDim.x) {
+    const uint32_t idx = base + threadIdx.x;
+    const uint32_t v = idx < ntiles ? b.tilesum[idx] : 0u;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t w = warp_tot[lane];
+      uint32_t wi = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= o) wi += t;
+      }
+      warp_tot[lane] = wi - w;
+    }
+    __syncthreads();
+    const uint32_t excl = carry + warp_tot[warp] + incl - v;
+    if (idx < ntiles) b.tilesum[idx] = excl;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) b.start[b.ncells] = carry;
+}
+
+__global__ void __launch_bounds__(256) k_scan_add(CellBufs b) {
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx < b.ncells) b.start[idx] += b.tilesum[idx / kScanTile];
+}
+
+__global__ void __launch_bounds__(256) k_scatter(CellBufs b) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= b.N) return;
+  b.pid_tmp[b.start[b.key[i]] + b.within[i]] = i;
+}
+
+// One warp per packed cell.  The rank of a member is the number of members
+// with a smaller particle id, which orders each cell canonically without
+// depending on the atomic tickets of k_bin.
+__global__ void __launch_bounds__(256) k_canon(CellBufs b) {
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= b.ncells) return;
+  const uint32_t s0 = b.start[warp], s1 = b.start[warp + 1];
+  const uint32_t n = s1 - s0;
+  if (n <= 32) {
+    const uint32_t me = lane < (int)n ? b.pid_tmp[s0 + lane] : kNone;
+    uint32_t rank = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+      const uint32_t other = __shfl_sync(0xffffffffu, me, k);
+      rank += other < me ? 1u : 0u;
+    }
+    if (lane < (int)n) {
+      const uint32_t s = s0 + rank;
+      b.pid[s] = me;
+      b.slot[me] = s;
+      const float4 p = b.r[me];
+      b.rs[s] = make_float4(p.x, p.y, p.z, __int_as_float((int)b.type[me]));
+    }
+  } else {
+    // Large cells: O(n^2 / 32) ranking straight from global memory.
+    for (uint32_t a = lane; a < n; a += 32) {
+      const uint32_t me = b.pid_tmp[s0 + a];
+      uint32_t rank = 0;
+      for (uint32_t k = 0; k < n; ++k) rank += b.pid_tmp[s0 + k] < me ? 1u : 0u;
+      const uint32_t s = s0 + rank;
+      b.pid[s] = me;
+      b.slot[me] = s;
+      const float4 p = b.r[me];
+      b.rs[s] = make_float4(p.x, p.y, p.z, __int_as_float((int)b.type[me]));
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_cell_build(const CellBufs &b, cudaStream_t s) {
+  if (b.N == 0) return cudaSuccess;
+  const uint32_t nb = (b.N + 255) / 256;
+  k_bin<<<nb, 256, 0, s>>>(b);
+  const uint32_t ntiles = (b.ncells + kScanTile - 1) / kScanTile;
+  k_scan_tiles<<<ntiles, 1024, 0, s>>>(b);
+  k_scan_top<<<1, 1024, 0, s>>>(b, ntiles);
+  k_scan_add<<<(b.ncells + 255) / 256, 256, 0, s>>>(b);
+  k_scatter<<<nb, 256, 0, s>>>(b);
+  const uint64_t canon_threads = (uint64_t)b.ncells * 32;
+  k_canon<<<(uint32_t)((canon_threads + 255) / 256), 256, 0, s>>>(b);
+  return cudaGetLastError();
+}
+
+}  // namespace pb

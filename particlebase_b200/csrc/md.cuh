@@ -1,0 +1,81 @@
+// Device data layout of one or many LJ systems packed into shared arrays, and
+// the kernel entry points that operate on them.
+//
+// Layout in HBM (all arrays in particle order unless noted):
+//   r      float4[N]   position x, y, z (w unused)           -- cudaParticleBase::r
+//   v      float4[N]   velocity (FP32 path), w = 0           -- cudaParticleBase::v
+//   vd     double[3N]  velocity, FP64, per-system SoA planes -- GaussianThermo::vd
+//   F[2]   float4[N]   force ping-pong: F[cur] is F(t), F[1-cur] is Fold
+//   minv   float[N]    1 / mass                               -- cudaParticleBase::minv
+//   type   uint16[N]   type id                                -- cudaParticleBase::typeID
+//   sysid  uint32[N]   owning system (batched mode only)
+// Cell list (rebuilt every step):
+//   key    uint32[N]   packed cell key of each atom: cell0 + rank(x,y) * nz + z
+//   start  uint32[C+1] first sorted slot of each packed cell (C = all cells)
+//   pid    uint32[N]   particle id at each sorted slot (cudaCutoffBlock::pid)
+//   slot   uint32[N]   sorted slot of each particle (inverse of pid)
+//   rs     float4[N]   sorted positions, w = type id bits (cudaSortedPositions::r_s)
+// Cell keys order the (x, y) columns of a box along a Morton (Z-order) curve and
+// keep z fastest, so the three z-adjacent cells of a column are contiguous.
+#pragma once
+
+#include "common.cuh"
+
+namespace pb {
+
+// One periodic system inside the packed arrays.
+struct SysDesc {
+  Grid g;
+  uint32_t atom0, natoms;   // particle range [atom0, atom0 + natoms)
+  uint32_t cell0;           // first packed cell key
+  uint32_t col0;            // offset of this system's column tables
+  uint32_t vd0;             // offset of this system's FP64 velocity planes (3 * atom0)
+  uint32_t lj;              // index of this system's LJ table
+  float dt;                 // time step
+  float pad;
+};
+
+// Work item of the force kernel: one (x, y) column of one system, z cells
+// [z0, z1).  Items are listed in column-Morton order.
+struct ForceItem {
+  uint32_t sys;
+  uint32_t col;     // column rank within the system
+  uint16_t z0, z1;
+};
+
+struct CellBufs {
+  const float4 *r;
+  const uint16_t *type;
+  const uint32_t *sysid;     // nullptr: every atom belongs to system 0
+  const SysDesc *sys;
+  const uint32_t *colrank;   // per system: reference column (d0 * ny + d1) -> rank
+  uint32_t N;
+  uint32_t ncells;           // packed cells over all systems
+  uint32_t *key, *within, *count, *start, *tilesum;
+  uint32_t *pid_tmp, *pid, *slot;
+  float4 *rs;
+  uint32_t *status;
+};
+
+struct ForceBufs {
+  const float4 *rs;
+  const uint32_t *start;     // packed cell starts
+  const uint32_t *pid;
+  const SysDesc *sys;
+  const uint32_t *colxy;     // per system: rank -> reference column (d0 * ny + d1)
+  const uint32_t *colrank;   // per system: reference column -> rank
+  const LJTable *lj;
+  const ForceItem *items;
+  uint32_t nitems;
+  int cap;                   // staged-atom capacity of a CTA's shared memory
+  float4 *F;                 // force output, particle order
+  double *partials;          // per-CTA energy partials (4 doubles per CTA)
+  uint32_t *status;
+};
+
+// Launchers (return cudaError_t of the launch).
+cudaError_t launch_cell_build(const CellBufs &b, cudaStream_t s);
+cudaError_t launch_force(const ForceBufs &b, int nt_max, bool energy, bool acc64,
+                         int block_threads, cudaStream_t s);
+
+}  // namespace pb

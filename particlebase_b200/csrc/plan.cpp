@@ -1,0 +1,96 @@
+#include "plan.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace pb {
+
+bool make_grid(const float cell6[6], float rmax, Grid &g) {
+  for (int i = 0; i < 3; ++i) {
+    const float c = cell6[2 * i + 1] - cell6[2 * i];
+    const float q = c / rmax;
+    if (!(q >= 3.0f) || q > 1.0e6f) return false;
+    g.n[i] = static_cast<int>(static_cast<uint32_t>(q));
+    g.len[i] = c / static_cast<float>(static_cast<uint32_t>(g.n[i]));
+    g.lo[i] = cell6[2 * i];
+    g.L[i] = c;
+  }
+  const uint64_t nc = (uint64_t)g.n[0] * g.n[1] * g.n[2];
+  if (nc >= 0xffffffffull) return false;
+  g.ncells = (uint32_t)nc;
+  return true;
+}
+
+static uint64_t spread_bits(uint32_t v) {
+  uint64_t x = v;
+  x = (x | (x << 16)) & 0x0000ffff0000ffffull;
+  x = (x | (x << 8)) & 0x00ff00ff00ff00ffull;
+  x = (x | (x << 4)) & 0x0f0f0f0f0f0f0f0full;
+  x = (x | (x << 2)) & 0x3333333333333333ull;
+  x = (x | (x << 1)) & 0x5555555555555555ull;
+  return x;
+}
+
+void morton_columns(int nx, int ny, std::vector<uint32_t> &rank, std::vector<uint32_t> &xy) {
+  const uint32_t nc = (uint32_t)nx * ny;
+  std::vector<std::pair<uint64_t, uint32_t>> code(nc);
+  for (int a = 0; a < nx; ++a)
+    for (int b = 0; b < ny; ++b) {
+      const uint32_t c = (uint32_t)a * ny + b;
+      code[c] = {spread_bits((uint32_t)a) | (spread_bits((uint32_t)b) << 1), c};
+    }
+  std::sort(code.begin(), code.end());
+  rank.assign(nc, 0);
+  xy.assign(nc, 0);
+  for (uint32_t k = 0; k < nc; ++k) {
+    rank[code[k].second] = k;
+    xy[k] = code[k].second;
+  }
+}
+
+void neighbor_table(const Grid &g, std::vector<uint32_t> &out) {
+  const long nx = g.n[0], ny = g.n[1], nz = g.n[2];
+  out.assign((size_t)g.ncells * 27, 0);
+  for (long i = 0; i < nx; ++i)
+    for (long j = 0; j < ny; ++j)
+      for (long k = 0; k < nz; ++k) {
+        const size_t I = (size_t)(k + j * nz + i * nz * ny);
+        int L = 0;
+        for (int a = -1; a <= 1; ++a)
+          for (int b = -1; b <= 1; ++b)
+            for (int c = -1; c <= 1; ++c) {
+              const long i2 = (i + a + nx) % nx, j2 = (j + b + ny) % ny, k2 = (k + c + nz) % nz;
+              out[I * 27 + L++] = (uint32_t)(k2 + j2 * nz + i2 * nz * ny);
+            }
+      }
+}
+
+int choose_segment(double atoms_per_cell, int nz) {
+  const double apc = std::max(atoms_per_cell, 1.0);
+  int seg = (int)std::ceil(160.0 / apc);
+  seg = std::max(1, std::min(seg, force_max_segment()));
+  return std::min(seg, nz);
+}
+
+int choose_capacity(double atoms_per_cell, int seg) {
+  const double expect = 9.0 * (seg + 2) * std::max(atoms_per_cell, 1.0);
+  const double cap = 1.5 * expect + 256.0;
+  const double max_atoms = (200.0 * 1024.0) / 16.0;
+  return (int)std::min(cap, max_atoms);
+}
+
+void append_items(uint32_t sys, const Grid &g, int seg, std::vector<ForceItem> &items) {
+  const uint32_t ncol = (uint32_t)g.n[0] * g.n[1];
+  for (uint32_t c = 0; c < ncol; ++c) {
+    for (int z = 0; z < g.n[2]; z += seg) {
+      ForceItem it;
+      it.sys = sys;
+      it.col = c;
+      it.z0 = (uint16_t)z;
+      it.z1 = (uint16_t)std::min(z + seg, g.n[2]);
+      items.push_back(it);
+    }
+  }
+}
+
+}  // namespace pb

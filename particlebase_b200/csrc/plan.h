@@ -1,0 +1,39 @@
+// Host-side planning shared by the single-system and batched paths:
+// the reference cell grid, Morton ranking of (x, y) columns and the force
+// work items.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "md.cuh"
+
+namespace pb {
+
+// cudaCutoffBlock::setupCutoffBlock, periodic branch (cudaCutoffBlock.cu:97-113),
+// in the same FP32 operations: blocknum = (uint32)(c / rmax),
+// blocklen = c / (float)blocknum.  Returns false if any axis has < 3 cells
+// (the reference asserts blocknum > 2).
+bool make_grid(const float cell6[6], float rmax, Grid &g);
+
+// rank[d0 * ny + d1] = position of column (d0, d1) along a Z-order curve;
+// xy[rank] = d0 * ny + d1.
+void morton_columns(int nx, int ny, std::vector<uint32_t> &rank, std::vector<uint32_t> &xy);
+
+// Reference 27-neighbour table (calc_BlockNeighbor, cudaCutoffBlock.cu:17-65),
+// periodic, in reference cell numbering d2 + d1 nz + d0 nz ny.
+void neighbor_table(const Grid &g, std::vector<uint32_t> &out);
+
+// z cells per force work item for a mean cell occupancy: about 160 home
+// atoms per CTA, at most kMaxSeg (see force.cu).
+int choose_segment(double atoms_per_cell, int nz);
+
+// Shared-memory capacity (atoms) of a force CTA staging 9 columns x (seg + 2)
+// cells at the given mean occupancy, with headroom for fluctuations.
+int choose_capacity(double atoms_per_cell, int seg);
+
+void append_items(uint32_t sys, const Grid &g, int seg, std::vector<ForceItem> &items);
+
+int force_max_segment();
+
+}  // namespace pb

@@ -1,0 +1,143 @@
+"""Generate golden vectors from the reference's own MD kernels.
+
+The reference (particlelover/ParticleBase) ships no unit tests or fixtures.
+This script runs its kernels -- compiled for the CPU into oracle/_ref by
+oracle/Makefile (calcBID_F4, the sortByBID family, makeBindex,
+calc_BlockNeighbor, calcF_IJpairWithBlock_F4<MDpairForce<potentialLJ>> +
+reduce27_F4, propagateVelocityVerlet_F4, the Gaussian-thermostat kernels and
+applyPeriodicCondition_F4) -- on small seeded inputs and stores the outputs in
+tests/golden/*.npz.  The oracle is checked against these files in
+tests/test_oracle.py, so the pin holds where the reference checkout is absent.
+
+    python tests/golden/make_golden.py      # needs oracle/_ref (make -C oracle ref)
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import pyoracle as po  # noqa: E402
+from particlebase_b200 import workloads as W  # noqa: E402
+
+
+def perturbed_c1(seed: int = 11, amp: float = 0.06):
+    s = W.config_c1(seed=1)
+    rng = np.random.default_rng(seed)
+    r = s.r + rng.uniform(-amp, amp, s.r.shape)
+    L = float(s.box[1])
+    r = np.mod(r, L)
+    r = np.minimum(r.astype(np.float32), np.nextafter(np.float32(L), np.float32(0)))
+    return s, r.astype(np.float64)
+
+
+def ref_system(s, r, gaussian=False, tol=1e-8):
+    return po.RefKernels(s.box, s.rc, r, s.v, s.mass, s.types, [1.0, 1.0], gaussian=gaussian,
+                         tol=tol)
+
+
+def main() -> None:
+    po.build(ref=True)
+    if not po.ref_available():
+        raise SystemExit("oracle/_ref is not built (needs the reference checkout)")
+    out = {}
+
+    # 1. cell table of C1 (4,000 fcc atoms, 6^3 cells), perturbed positions
+    s, r = perturbed_c1()
+    R = ref_system(s, r)
+    R.calc_block_id()
+    bid, pid, bindex = R.cells()
+    cell_of = np.empty(s.n, np.uint32)
+    cell_of[pid] = bid
+    n3, blocklen = R.grid()
+    out.update(c1_box=s.box, c1_r4=R.get4("r"), c1_cell_of=cell_of, c1_blocknum=n3,
+               c1_blocklen=blocklen[:3], c1_neighbors=R.neighbors(),
+               c1_v=s.v.astype(np.float32))
+
+    # 2. forces of the same snapshot (FP32 reference kernel)
+    R.calc_force()
+    out["c1_F"] = R.get4("F")
+
+    # 3. 10 velocity-Verlet steps (calcBlockID, calcForce, TimeEvolution, wrap)
+    R2 = ref_system(s, r)
+    R2.run(0.005, 10)
+    out["c1_vv10_r4"] = R2.get4("r")
+    out["c1_vv10_v4"] = R2.get4("v")
+
+    # 4. 10 Gaussian-thermostat steps at the reference's default Newton-Raphson
+    # tolerance (GaussianThermo() : _e(1e-8)).  With 1e-10, as testMD2 sets,
+    # the FP32/FP64 mix of the reference kernels stalls at step 9 of this run
+    # and the reference would exit(0) (GaussianThermo.cu:42-45).
+    R3 = ref_system(s, r, gaussian=True)
+    if R3.run(0.005, 10) < 0:
+        raise SystemExit("reference Newton-Raphson did not converge")
+    out["c1_gauss10_r4"] = R3.get4("r")
+    out["c1_gauss10_vd"] = R3.vd()
+    out["c1_gauss10_xi"] = np.array([R3.xi])
+
+    # 5. two-body forces in a 10 x 10 x 10 box along x, y and z.  The first
+    # atom sits in cell 0: makeBindex sets bindex[0] = 0 unconditionally
+    # (kernelfuncs.cu:896), so with cell 0 empty the reference would file the
+    # first occupied cell's atoms under cell 0 (see item 8).
+    dists = np.array([0.9, 2 ** (1 / 6), 1.5, 2.49, 2.51], np.float64)
+    box = np.array([0, 10, 0, 10, 0, 10], np.float32)
+    pair_F = []
+    for d in dists:
+        for axis in range(3):
+            rr = np.full((2, 3), 0.5)
+            rr[1, axis] += d
+            Rp = po.RefKernels(box, 2.5, rr, np.zeros((2, 3)), np.ones(2), np.zeros(2, np.uint32),
+                               [1.0, 1.0])
+            Rp.calc_block_id()
+            Rp.calc_force()
+            pair_F.append(Rp.get4("F"))
+    out["pair_dist"] = dists
+    out["pair_F"] = np.stack(pair_F)
+
+    # 6. minimum image across each face: a pair straddling x, y, z = 0
+    img_F = []
+    for axis in range(3):
+        rr = np.full((2, 3), 0.3)
+        rr[1, axis] = 9.5   # nearest image of atom 1 is at -0.5: distance 0.8
+        Rp = po.RefKernels(box, 2.5, rr, np.zeros((2, 3)), np.ones(2), np.zeros(2, np.uint32),
+                           [1.0, 1.0])
+        Rp.calc_block_id()
+        Rp.calc_force()
+        img_F.append(Rp.get4("F"))
+    out["image_F"] = np.stack(img_F)
+
+    # 7. periodic wrap of out-of-box FP32 coordinates
+    rng = np.random.default_rng(5)
+    rw = rng.uniform(-25.0, 35.0, (256, 3))
+    Rw = po.RefKernels(box, 2.5, rw, np.zeros((256, 3)), np.ones(256), np.zeros(256, np.uint32),
+                       [1.0, 1.0])
+    out["wrap_box"] = box
+    out["wrap_in"] = Rw.get4("r")
+    Rw.wrap()
+    out["wrap_out"] = Rw.get4("r")
+
+    # 8. the makeBindex quirk itself: the same pair as item 6 (x axis) moved to
+    # y = z = 5 leaves cell 0 empty; the reference then returns zero force.
+    rr = np.full((2, 3), 5.0)
+    rr[0, 0] = 0.3
+    rr[1, 0] = 9.5
+    Rq = po.RefKernels(box, 2.5, rr, np.zeros((2, 3)), np.ones(2), np.zeros(2, np.uint32),
+                       [1.0, 1.0])
+    Rq.calc_block_id()
+    Rq.calc_force()
+    out["quirk_r"] = rr
+    out["quirk_F"] = Rq.get4("F")
+
+    path = os.path.join(HERE, "reference_kernels.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "bytes")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,214 @@
+"""Pins of the FP64 oracle (CPU only).
+
+The reference has no tests or fixtures of its own, so the oracle is pinned
+two ways: against golden vectors produced by the reference's own kernels
+(tests/golden/reference_kernels.npz, made by tests/golden/make_golden.py from
+oracle/_ref), and, where the reference checkout is present, against those
+kernels directly on further inputs.  Plus known answers: analytic two-body
+forces, the zero net force of a perfect fcc lattice, momentum conservation.
+"""
+import numpy as np
+import pytest
+
+from particlebase_b200 import workloads as W
+
+
+def relrms(a, b):
+    return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+
+def lj_force_analytic(r, sigma=1.0, eps=1.0):
+    return 24 * eps * (2 * (sigma / r) ** 12 - (sigma / r) ** 6) / r
+
+
+def test_grid_matches_reference(po, golden):
+    n, ln = po.grid(golden["c1_box"], 2.5)
+    assert np.array_equal(n, golden["c1_blocknum"])
+    assert np.array_equal(ln, golden["c1_blocklen"])  # bit-exact FP32 blocklen
+
+
+def test_cell_of_matches_reference(po, golden):
+    cid = po.bin_cells(golden["c1_r4"], golden["c1_box"], 2.5)
+    assert np.array_equal(cid, golden["c1_cell_of"])
+
+
+def test_neighbor_table_matches_reference(po, golden):
+    assert np.array_equal(po.neighbor_table(golden["c1_box"], 2.5), golden["c1_neighbors"])
+
+
+def test_cell_list_is_stable_counting_sort(po):
+    rng = np.random.default_rng(0)
+    cid = rng.integers(0, 50, 1000).astype(np.uint32)
+    start, members = po.cell_list(cid, 50)
+    assert start[-1] == 1000
+    for c in range(50):
+        m = members[start[c]:start[c + 1]]
+        assert np.all(cid[m] == c)
+        assert np.all(np.diff(m.astype(np.int64)) > 0)  # ascending particle id
+
+
+def test_forces_match_reference_kernel(po, golden):
+    r4 = golden["c1_r4"]
+    O = po.Oracle(golden["c1_box"], W.single_type_lj(), 2.5, r4[:, :3].astype(np.float64))
+    info = O.forces()
+    F = O.get("F")
+    Fr = golden["c1_F"][:, :3].astype(np.float64)
+    L = float(golden["c1_box"][1])
+    x = r4[:, :3]
+    interior = np.all((x > 2.5) & (x < L - 2.5), axis=1)
+    # Away from the faces the FP32 reference kernel and the FP64 oracle agree to
+    # FP32 rounding.  Near the faces the reference's minimum image in r^2,
+    # dx^2 + 4 (c - sqrt(c dx^2)) (kernelinline.hh:47-62), cancels and costs it
+    # about two decimal digits, hence the looser whole-system bound.
+    assert relrms(Fr[interior], F[interior]) < 2e-6
+    assert relrms(Fr, F) < 1e-4
+    assert info["ncand"] == 4000 * (27 * 4000 / 216 - 1)
+    assert np.abs(F.sum(0)).max() < 1e-9  # Newton's third law in aggregate
+
+
+def test_pair_forces_analytic_and_reference(po, golden):
+    box = np.array([0, 10, 0, 10, 0, 10], np.float32)
+    k = 0
+    for d in golden["pair_dist"]:
+        for axis in range(3):
+            rr = np.full((2, 3), 0.5)
+            rr[1, axis] += d
+            O = po.Oracle(box, W.single_type_lj(), 2.5, rr)
+            O.forces()
+            F = O.get("F")
+            expect = lj_force_analytic(d) if d < 2.5 else 0.0
+            assert F[0, axis] == pytest.approx(-expect, rel=1e-12, abs=1e-15)
+            assert F[1, axis] == pytest.approx(expect, rel=1e-12, abs=1e-15)
+            Fr = golden["pair_F"][k][:, :3]
+            # FP32 reference: at the force minimum r = 2^(1/6) the factor
+            # 2 (s/r)^6 - 1 cancels, so the absolute bound is on the force
+            # scale 24 eps / sigma.
+            assert np.allclose(F, Fr, rtol=2e-6, atol=24 * 2e-6)
+            k += 1
+
+
+def test_minimum_image_across_faces(po, golden):
+    box = np.array([0, 10, 0, 10, 0, 10], np.float32)
+    for axis in range(3):
+        rr = np.full((2, 3), 0.3)
+        rr[1, axis] = 9.5
+        O = po.Oracle(box, W.single_type_lj(), 2.5, rr)
+        O.forces()
+        F = O.get("F")
+        f = lj_force_analytic(0.8)
+        assert F[0, axis] == pytest.approx(f, rel=1e-12)  # pushed away from the image at -0.5
+        # FP32 reference through its sqrt-based image distance: ~1e-4 relative
+        assert np.allclose(F, golden["image_F"][axis][:, :3], rtol=3e-4)
+
+
+def test_reference_empty_cell0_quirk_is_not_reproduced(po, golden):
+    """makeBindex writes bindex[0] = 0 unconditionally (kernelfuncs.cu:896):
+    with cell 0 empty the reference misfiles the first occupied cell and this
+    pair gets no force.  The oracle (and the CUDA path) use correct cell ranges."""
+    assert np.all(golden["quirk_F"][:, :3] == 0)
+    box = np.array([0, 10, 0, 10, 0, 10], np.float32)
+    O = po.Oracle(box, W.single_type_lj(), 2.5, golden["quirk_r"])
+    O.forces()
+    assert O.get("F")[0, 0] == pytest.approx(lj_force_analytic(0.8), rel=1e-12)
+
+
+def test_wrap_bit_exact_with_reference(po, golden):
+    w = po.wrap_f32(golden["wrap_in"], golden["wrap_box"])
+    assert np.array_equal(w[:, :3], golden["wrap_out"][:, :3])
+
+
+def test_vv_trajectory_matches_reference(po, golden):
+    r4 = golden["c1_r4"]
+    box = golden["c1_box"]
+    L = float(box[1])
+    O = po.Oracle(box, W.single_type_lj(), 2.5, r4[:, :3].astype(np.float64),
+                  golden["c1_v"].astype(np.float64))
+    O.run(10, 0.005)
+    d = O.get("r") - golden["c1_vv10_r4"][:, :3]
+    d -= L * np.round(d / L)
+    assert np.abs(d).max() < 2e-5
+    assert np.abs(O.get("v") - golden["c1_vv10_v4"][:, :3]).max() < 2e-4
+
+
+def test_gaussian_trajectory_matches_reference(po, golden):
+    r4 = golden["c1_r4"]
+    box = golden["c1_box"]
+    L = float(box[1])
+    O = po.Oracle(box, W.single_type_lj(), 2.5, r4[:, :3].astype(np.float64),
+                  golden["c1_v"].astype(np.float64))
+    O.set_tol(1e-8)
+    O.run(10, 0.005, mode="gauss")
+    d = O.get("r") - golden["c1_gauss10_r4"][:, :3]
+    d -= L * np.round(d / L)
+    assert np.abs(d).max() < 2e-5
+    assert np.abs(O.get("v") - golden["c1_gauss10_vd"]).max() < 2e-4
+    assert O.xi == pytest.approx(float(golden["c1_gauss10_xi"][0]), rel=1e-5)
+
+
+def test_gaussian_holds_kinetic_energy(po):
+    # The discrete isokinetic scheme of GaussianThermo keeps sum m v^2 to
+    # O(dt^2) per step, not exactly; the reference kernels show the same drift.
+    s = W.config_c1()
+    O = po.Oracle(s.box, s.lj, s.rc, s.r, s.v)
+    O.set_tol(1e-12)
+    k0 = O.kinetic()
+    O.run(20, 0.005, mode="gauss")
+    assert O.kinetic() == pytest.approx(k0, rel=5e-3)
+
+
+def test_gaussian_closed_form_equals_newton_raphson(po):
+    """xi = c / (1 - c dt/2) with c = sum F.A / sum m A^2 is the fixed point
+    the reference's Newton-Raphson loop converges to (GaussianThermo.cu:29-77)."""
+    s = W.config_c1()
+    dt = 0.005
+    O = po.Oracle(s.box, s.lj, s.rc, s.r, s.v)
+    O.set_tol(1e-13)
+    O.run(3, dt, mode="gauss")  # arbitrary state with nonzero Fold, xi
+    v0, xi0, fold = O.get("v"), O.xi, O.get("Fold")
+    O.forces()
+    F = O.get("F")
+    A = v0 + (F + fold) * dt / 2 - v0 * xi0 * dt / 2
+    c = (F * A).sum() / (A * A).sum()
+    xi = c / (1 - c * dt / 2)
+    O.run(1, dt, mode="gauss")
+    assert O.xi == pytest.approx(xi, rel=1e-10)
+    assert np.allclose(O.get("v"), A / (1 + xi * dt / 2), rtol=1e-10, atol=1e-12)
+
+
+def test_fcc_lattice_has_zero_force(po):
+    s = W.fcc_system(6, 0.8442, 0.0 + 1e-9, seed=0)
+    O = po.Oracle(s.box, s.lj, s.rc, s.r)
+    O.forces()
+    assert np.abs(O.get("F")).max() < 1e-10
+
+
+def test_nve_conserves_shifted_energy(po):
+    # Truncated-force dynamics conserve KE + sum (U(r) - U(rc)); the first step
+    # is skipped because Fold = 0 there (cudaParticleVV::clearForce) gives the
+    # reference scheme a one-off double force kick.
+    s = W.config_c1()
+    O = po.Oracle(s.box, s.lj, s.rc, s.r, s.v)
+    e = O.run(400, 0.005, record=True)[1:]
+    etot = (e[:, 0] + e[:, 2]) / s.n
+    drift = np.polyfit(np.arange(len(etot)), etot, 1)[0] * 1000
+    assert abs(drift) < 1e-4
+    assert np.std(etot) < 2e-4
+
+
+@pytest.mark.skipif("not __import__('pyoracle').ref_available()")
+def test_kob_andersen_forces_vs_reference_kernel(po):
+    """Two-type system with one global cutoff (the reference has no per-pair rc)."""
+    s = W.kob_andersen_random(3000, 1.2, 0.8, seed=3)
+    O = po.Oracle(s.box, s.lj, s.rc, s.r, s.v, types=s.types)
+    O.steepest_descent(30, 0.02)
+    r = O.get("r")
+    lj_global = s.lj.copy()
+    lj_global[..., 2] = 2.5
+    O2 = po.Oracle(s.box, lj_global, 2.5, r.astype(np.float32).astype(np.float64), types=s.types)
+    O2.forces()
+    R = po.RefKernels(s.box, 2.5, r, s.v, s.mass, s.types, s.lj[..., :2].reshape(-1), ntypes=2)
+    R.calc_block_id()
+    R.calc_force()
+    F = O2.get("F")
+    Fr = R.get4("F")[:, :3].astype(np.float64)
+    assert relrms(Fr, F) < 2e-4
