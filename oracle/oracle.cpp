@@ -102,17 +102,25 @@ void neighbor_table(const Grid &g, int periodic, uint32_t *out) {
       }
 }
 
-// Counting sort of atoms by cell id, stable in particle id.  Replaces the
-// reference's racy single-CTA sort (sortByBID_M1 + sortByBID + makeBindex,
-// kernelfuncs.cu:844-932): the per-cell member sets and counts are the same,
-// the within-cell order is made canonical (ascending particle id).
-void cell_list(const uint32_t *cid, uint32_t N, uint32_t ncells, uint32_t *start,
-               uint32_t *members) {
+// Counting sort of atoms by cell id.  Replaces the reference's racy
+// single-CTA sort (sortByBID_M1 + sortByBID + makeBindex,
+// kernelfuncs.cu:844-932): the per-cell member sets and counts are the same;
+// the within-cell order, history-dependent in the reference, is made
+// canonical: ascending FP32 z coordinate, ties by ascending particle id.
+// `z` may be null, giving ascending particle id.
+void cell_list(const uint32_t *cid, const float *z, uint32_t N, uint32_t ncells,
+               uint32_t *start, uint32_t *members) {
   std::vector<uint32_t> cnt(ncells + 1, 0);
   for (uint32_t i = 0; i < N; ++i) cnt[cid[i] + 1]++;
   for (uint32_t c = 0; c < ncells; ++c) cnt[c + 1] += cnt[c];
   std::memcpy(start, cnt.data(), sizeof(uint32_t) * (ncells + 1));
   for (uint32_t i = 0; i < N; ++i) members[cnt[cid[i]]++] = i;
+  if (z) {
+    for (uint32_t c = 0; c < ncells; ++c)
+      std::sort(members + start[c], members + start[c + 1], [z](uint32_t a, uint32_t b) {
+        return z[a] < z[b] || (z[a] == z[b] && a < b);
+      });
+  }
 }
 
 struct LJTable {
@@ -240,7 +248,7 @@ void build_cells(System &s) {
     // The reference bins the FP32 copy of the position (float4 r).
     cid[i] = cell_of(s.g, (float)s.r[3 * i], (float)s.r[3 * i + 1], (float)s.r[3 * i + 2]);
   }
-  cell_list(cid.data(), s.N, s.g.ncells, s.start.data(), s.members.data());
+  cell_list(cid.data(), nullptr, s.N, s.g.ncells, s.start.data(), s.members.data());
 }
 
 void forces(System &s) {
@@ -376,9 +384,9 @@ int orc_bin(const float *r4, uint32_t N, const float *cell6, float rc, uint32_t 
   return 0;
 }
 
-int orc_cell_list(const uint32_t *cid, uint32_t N, uint32_t ncells, uint32_t *start,
-                  uint32_t *members) {
-  cell_list(cid, N, ncells, start, members);
+int orc_cell_list(const uint32_t *cid, const float *z, uint32_t N, uint32_t ncells,
+                  uint32_t *start, uint32_t *members) {
+  cell_list(cid, z, N, ncells, start, members);
   return 0;
 }
 

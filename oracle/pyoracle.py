@@ -57,7 +57,7 @@ def lib() -> C.CDLL:
         L.orc_grid.argtypes = [_f32p, C.c_float, _u32p, _f32p]
         L.orc_neighbor_table.argtypes = [_f32p, C.c_float, C.c_int, _u32p]
         L.orc_bin.argtypes = [_f32p, C.c_uint32, _f32p, C.c_float, _u32p]
-        L.orc_cell_list.argtypes = [_u32p, C.c_uint32, C.c_uint32, _u32p, _u32p]
+        L.orc_cell_list.argtypes = [_u32p, C.c_void_p, C.c_uint32, C.c_uint32, _u32p, _u32p]
         L.orc_wrap_f32.argtypes = [_f32p, C.c_uint32, _f32p]
         L.orc_create.restype = C.c_void_p
         L.orc_create.argtypes = [C.c_uint32, _f32p, C.c_float, _f64p, C.c_int]
@@ -148,11 +148,14 @@ def bin_cells(r4, box, rc):
     return out
 
 
-def cell_list(cid, ncells):
+def cell_list(cid, ncells, z=None):
+    """Members per cell; within a cell by ascending FP32 z (ties: particle id)
+    when z is given, else by particle id."""
     cid = np.ascontiguousarray(cid, np.uint32)
     start = np.zeros(ncells + 1, np.uint32)
     members = np.zeros(len(cid), np.uint32)
-    lib().orc_cell_list(cid, len(cid), ncells, start, members)
+    zz = None if z is None else np.ascontiguousarray(z, np.float32)
+    lib().orc_cell_list(cid, None if zz is None else zz.ctypes.data, len(cid), ncells, start, members)
     return start, members
 
 

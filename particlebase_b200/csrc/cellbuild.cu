@@ -6,15 +6,17 @@
 // sortByBID_M1, the single-CTA sortByBID, makeBindex and copyWithIndex
 // (kernelfuncs.cu:807-932).  The cell of each atom is computed with the same
 // FP32 arithmetic as calcBID_F4, so cell membership is bit-identical; the
-// within-cell order is canonical (ascending particle id) instead of the
-// reference's history-dependent order.
+// within-cell order is canonical -- ascending z, ties by particle id -- instead
+// of the reference's history-dependent order.  Because the cell index is a
+// monotone function of z, every (x, y) column of cells is then sorted by z,
+// which the force kernel uses to cut z windows by binary search.
 //
 // Kernels, in launch order:
 //   k_bin       read r (16 B/atom), write key + within-cell ticket (8 B/atom)
 //   k_scan_*    exclusive scan of per-cell counts -> start[], zero the counts
 //   k_scatter   pid_tmp[start[key] + ticket] = i
-//   k_canon     one warp per cell: order members by particle id, write pid,
-//               slot and the sorted position float4 (type id in .w)
+//   k_canon     one warp per cell: order members by (z, particle id), write
+//               pid, slot and the sorted position float4 (type id in .w)
 #include "md.cuh"
 
 namespace pb {
@@ -134,9 +136,13 @@ __global__ void __launch_bounds__(256) k_scatter(CellBufs b) {
   b.pid_tmp[b.start[b.key[i]] + b.within[i]] = i;
 }
 
+__device__ __forceinline__ bool canon_before(float za, uint32_t a, float zb, uint32_t b) {
+  return za < zb || (za == zb && a < b);
+}
+
 // One warp per packed cell.  The rank of a member is the number of members
-// with a smaller particle id, which orders each cell canonically without
-// depending on the atomic tickets of k_bin.
+// before it in (z, particle id) order, which orders each cell canonically
+// without depending on the atomic tickets of k_bin.
 __global__ void __launch_bounds__(256) k_canon(CellBufs b) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -145,28 +151,32 @@ __global__ void __launch_bounds__(256) k_canon(CellBufs b) {
   const uint32_t n = s1 - s0;
   if (n <= 32) {
     const uint32_t me = lane < (int)n ? b.pid_tmp[s0 + lane] : kNone;
+    const float4 p = lane < (int)n ? b.r[me] : make_float4(0.f, 0.f, 0.f, 0.f);
     uint32_t rank = 0;
     for (uint32_t k = 0; k < n; ++k) {
       const uint32_t other = __shfl_sync(0xffffffffu, me, k);
-      rank += other < me ? 1u : 0u;
+      const float zo = __shfl_sync(0xffffffffu, p.z, k);
+      rank += canon_before(zo, other, p.z, me) ? 1u : 0u;
     }
     if (lane < (int)n) {
       const uint32_t s = s0 + rank;
       b.pid[s] = me;
       b.slot[me] = s;
-      const float4 p = b.r[me];
       b.rs[s] = make_float4(p.x, p.y, p.z, __int_as_float((int)b.type[me]));
     }
   } else {
     // Large cells: O(n^2 / 32) ranking straight from global memory.
     for (uint32_t a = lane; a < n; a += 32) {
       const uint32_t me = b.pid_tmp[s0 + a];
+      const float4 p = b.r[me];
       uint32_t rank = 0;
-      for (uint32_t k = 0; k < n; ++k) rank += b.pid_tmp[s0 + k] < me ? 1u : 0u;
+      for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t other = b.pid_tmp[s0 + k];
+        rank += canon_before(b.r[other].z, other, p.z, me) ? 1u : 0u;
+      }
       const uint32_t s = s0 + rank;
       b.pid[s] = me;
       b.slot[me] = s;
-      const float4 p = b.r[me];
       b.rs[s] = make_float4(p.x, p.y, p.z, __int_as_float((int)b.type[me]));
     }
   }

@@ -19,6 +19,12 @@
 // xi = c / (1 - c dt/2).  This is the fixed point the reference iterates
 // towards (it stops within its tolerance of it), computed on the device in
 // two passes with no host round trip.
+//
+// One case differs: the reference tests convergence with the xi of the
+// previous iteration, and when xi(t-dt) is exactly 0 (the first step after
+// construction) its initial guess v = A already gives f = 0, so the loop ends
+// after one pass with v = A and xi = sum F.A / sum m A^2 = c.  That step is
+// reproduced as the reference computes it.
 #include "integrate.cuh"
 
 namespace pb {
@@ -109,7 +115,7 @@ __global__ void __launch_bounds__(kThreads) k_gauss_a(IntegrateArgs a) {
   if (last_block_total<2>(s, a.partials, &a.sc->counter[1], tot, red)) {
     const double hdt = 0.5 * (double)a.dt;
     const double c = tot[1] > 0 ? tot[0] / tot[1] : 0.0;
-    double xi = c / (1.0 - c * hdt);
+    double xi = (xi_old == 0.0) ? c : c / (1.0 - c * hdt);
     if (!isfinite(xi) || !isfinite(tot[0]) || !isfinite(tot[1])) {
       atomicOr(a.status, kStatusNonFinite | kStatusNoConverge);
       xi = 0.0;
@@ -131,7 +137,7 @@ __global__ void __launch_bounds__(kThreads) k_gauss_b(IntegrateArgs a) {
     float4 F;
     gauss_A(a, i, xi_old, A, F);
     const double dt = a.dt;
-    const double inv = 1.0 / (1.0 + xi * 0.5 * dt);
+    const double inv = (xi_old == 0.0) ? 1.0 : 1.0 / (1.0 + xi * 0.5 * dt);
     const double v[3] = {A[0] * inv, A[1] * inv, A[2] * inv};
     const double cv = dt - xi * 0.5 * dt * dt;
     const double cf = 0.5 * dt * dt * (double)a.minv[i];

@@ -36,11 +36,16 @@ struct SysDesc {
 };
 
 // Work item of the force kernel: one (x, y) column of one system, z cells
-// [z0, z1).  Items are listed in column-Morton order.
+// [z0, z1).  Items are listed in column-Morton order.  The packed key of z cell
+// 0 of the 3 x 3 neighbour columns (x offset outer, y offset inner, each
+// -1, 0, +1, periodic) is precomputed on the host, so a CTA's first global
+// loads are the cell starts it stages.
 struct ForceItem {
   uint32_t sys;
-  uint32_t col;     // column rank within the system
+  uint32_t col;         // column rank within the system
   uint16_t z0, z1;
+  uint16_t cx, cy;      // column coordinates (frame shifts on the top faces)
+  uint32_t kbase[9];
 };
 
 struct CellBufs {

@@ -1,5 +1,6 @@
 // Host implementation of the single-system C ABI (include/pb/pb.h).
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
@@ -35,6 +36,7 @@ struct pb_md {
   bool cells_ready = false;
   double m0 = 1.0;
   int seg = 1, cap = 0;
+  int force_threads = 256;
   std::vector<uint32_t> key_of_ref;   // reference cell id -> key
   std::vector<uint32_t> ref_of_key;   // key -> reference cell id
 
@@ -188,8 +190,8 @@ int do_build(pb_md *h) {
 }
 
 int do_force(pb_md *h, bool energy) {
-  cudaError_t e = launch_force(fbufs(h), h->lj.nt, energy, (h->flags & PB_MD_ACC_FP64) != 0, 128,
-                               h->stream);
+  cudaError_t e = launch_force(fbufs(h), h->lj.nt, energy, (h->flags & PB_MD_ACC_FP64) != 0,
+                               h->force_threads, h->stream);
   if (e != cudaSuccess) return cuda_fail(h, e, "force");
   if (energy) {
     e = launch_energy_total(h->fpartials, h->nitems, h->sc, h->stream);
@@ -471,11 +473,12 @@ int pb_md_setup_cells(pb_md *h, float rmax, int periodic) {
   const uint32_t N = h->N, C = g.ncells;
   const double apc = (double)N / C;
   h->seg = choose_segment(apc, g.n[2]);
+  if (const char *e = std::getenv("PB_FORCE_THREADS")) h->force_threads = std::atoi(e);
   h->cap = choose_capacity(apc, h->seg);
   std::vector<uint32_t> rank, xy;
   morton_columns(g.n[0], g.n[1], rank, xy);
   std::vector<ForceItem> items;
-  append_items(0, g, h->seg, items);
+  append_items(0, g, h->seg, 0, rank, xy, items);
   h->nitems = (uint32_t)items.size();
   // key <-> reference cell id maps
   h->key_of_ref.assign(C, 0);

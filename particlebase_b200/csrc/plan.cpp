@@ -2,6 +2,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 namespace pb {
 
@@ -66,30 +67,57 @@ void neighbor_table(const Grid &g, std::vector<uint32_t> &out) {
 }
 
 int choose_segment(double atoms_per_cell, int nz) {
+  // about 160 home atoms (20 clusters of 8) per force CTA; PB_FORCE_SEG overrides
   const double apc = std::max(atoms_per_cell, 1.0);
-  int seg = (int)std::ceil(160.0 / apc);
+  int seg = (int)std::lround(160.0 / apc);
+  if (const char *e = std::getenv("PB_FORCE_SEG")) seg = std::atoi(e);
   seg = std::max(1, std::min(seg, force_max_segment()));
   return std::min(seg, nz);
 }
 
 int choose_capacity(double atoms_per_cell, int seg) {
   const double expect = 9.0 * (seg + 2) * std::max(atoms_per_cell, 1.0);
-  const double cap = 1.5 * expect + 256.0;
-  const double max_atoms = (200.0 * 1024.0) / 16.0;
+  double factor = 1.15;  // headroom over the mean occupancy; PB_FORCE_CAP overrides
+  if (const char *e = std::getenv("PB_FORCE_CAP")) factor = std::atof(e);
+  const double cap = factor * expect + 128.0;
+  const double max_atoms = (190.0 * 1024.0) / 16.0;
   return (int)std::min(cap, max_atoms);
 }
 
-void append_items(uint32_t sys, const Grid &g, int seg, std::vector<ForceItem> &items) {
+// z runs of one column: a top run of t <= nz/2 - 1 cells (its staged cells,
+// from z0 - 1 up, then all lie at z >= L/2, where the force kernel's frame
+// shift by -L is exact), the rest split evenly into runs of at most `seg`.
+// Every column gets at least two runs, so no run touches both faces.
+void append_items(uint32_t sys, const Grid &g, int seg, uint32_t cell0,
+                  const std::vector<uint32_t> &rank, const std::vector<uint32_t> &xy,
+                  std::vector<ForceItem> &items) {
   const uint32_t ncol = (uint32_t)g.n[0] * g.n[1];
+  const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+  const int t = std::max(1, std::min(seg, nz / 2 - 1));
+  const int rest = nz - t;
+  const int parts = std::max(1, (rest + seg - 1) / seg);
   for (uint32_t c = 0; c < ncol; ++c) {
-    for (int z = 0; z < g.n[2]; z += seg) {
-      ForceItem it;
-      it.sys = sys;
-      it.col = c;
-      it.z0 = (uint16_t)z;
-      it.z1 = (uint16_t)std::min(z + seg, g.n[2]);
-      items.push_back(it);
+    ForceItem it{};
+    it.sys = sys;
+    it.col = c;
+    const int cx = (int)(xy[c] / (uint32_t)ny), cy = (int)(xy[c] % (uint32_t)ny);
+    it.cx = (uint16_t)cx;
+    it.cy = (uint16_t)cy;
+    for (int k = 0; k < 9; ++k) {
+      const int ax = (cx + k / 3 - 1 + nx) % nx, ay = (cy + k % 3 - 1 + ny) % ny;
+      it.kbase[k] = cell0 + rank[(size_t)ax * ny + ay] * (uint32_t)nz;
     }
+    int z = 0;
+    for (int p = 0; p < parts; ++p) {
+      const int len = rest / parts + (p < rest % parts ? 1 : 0);
+      it.z0 = (uint16_t)z;
+      it.z1 = (uint16_t)(z + len);
+      items.push_back(it);
+      z += len;
+    }
+    it.z0 = (uint16_t)rest;
+    it.z1 = (uint16_t)nz;
+    items.push_back(it);
   }
 }
 

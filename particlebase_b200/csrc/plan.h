@@ -32,7 +32,11 @@ int choose_segment(double atoms_per_cell, int nz);
 // cells at the given mean occupancy, with headroom for fluctuations.
 int choose_capacity(double atoms_per_cell, int seg);
 
-void append_items(uint32_t sys, const Grid &g, int seg, std::vector<ForceItem> &items);
+// Force work items of one system whose packed cell keys start at cell0, with
+// the column ranking `rank` (reference column -> rank) and its inverse `xy`.
+void append_items(uint32_t sys, const Grid &g, int seg, uint32_t cell0,
+                  const std::vector<uint32_t> &rank, const std::vector<uint32_t> &xy,
+                  std::vector<ForceItem> &items);
 
 int force_max_segment();
 

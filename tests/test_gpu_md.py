@@ -53,12 +53,12 @@ def check_cells(p, s, po):
     pid = p.get("pid")
     assert start[-1] == s.n
     assert np.array_equal(np.sort(pid), np.arange(s.n))
-    ostart, omem = po.cell_list(cid, C)
+    ostart, omem = po.cell_list(cid, C, r4[:, 2])
     for ref in range(C):
         k = key[ref]
         got = pid[start[k]:start[k + 1]]
         exp = omem[ostart[ref]:ostart[ref + 1]]
-        assert np.array_equal(got, exp), f"members of cell {ref}"  # same set, same order
+        assert np.array_equal(got, exp), f"members of cell {ref}"  # same set, same z order
     rs = p.get("r_sorted")
     assert np.array_equal(rs[:, :3].view(np.uint32), r4[pid, :3].view(np.uint32))
     assert np.array_equal(rs[:, 3].view(np.int32), s.types[pid].astype(np.int32))

@@ -47,6 +47,18 @@ def test_cell_list_is_stable_counting_sort(po):
         assert np.all(np.diff(m.astype(np.int64)) > 0)  # ascending particle id
 
 
+def test_cell_list_orders_by_z_then_id(po):
+    rng = np.random.default_rng(1)
+    cid = rng.integers(0, 20, 2000).astype(np.uint32)
+    z = rng.integers(0, 30, 2000).astype(np.float32) * np.float32(0.25)  # many ties
+    start, members = po.cell_list(cid, 20, z)
+    for c in range(20):
+        m = members[start[c]:start[c + 1]]
+        assert np.all(cid[m] == c)
+        key = list(zip(z[m].tolist(), m.tolist()))
+        assert key == sorted(key)
+
+
 def test_forces_match_reference_kernel(po, golden):
     r4 = golden["c1_r4"]
     O = po.Oracle(golden["c1_box"], W.single_type_lj(), 2.5, r4[:, :3].astype(np.float64))
@@ -173,6 +185,21 @@ def test_gaussian_closed_form_equals_newton_raphson(po):
     O.run(1, dt, mode="gauss")
     assert O.xi == pytest.approx(xi, rel=1e-10)
     assert np.allclose(O.get("v"), A / (1 + xi * dt / 2), rtol=1e-10, atol=1e-12)
+
+
+def test_gaussian_first_step_stops_after_one_iteration(po):
+    """With xi(t-dt) = 0 the reference's initial guess v = A satisfies its
+    convergence test at once: v = A and xi = sum F.A / sum m A^2."""
+    s = W.config_c1()
+    dt = 0.005
+    O = po.Oracle(s.box, s.lj, s.rc, s.r, s.v)
+    O.set_tol(1e-13)
+    O.forces()
+    F = O.get("F")
+    A = s.v + F * dt / 2
+    O.run(1, dt, mode="gauss")
+    assert O.xi == pytest.approx((F * A).sum() / (A * A).sum(), rel=1e-12)
+    assert np.allclose(O.get("v"), A, rtol=1e-12, atol=1e-14)
 
 
 def test_fcc_lattice_has_zero_force(po):
