@@ -203,6 +203,27 @@ int pb_plan_columns(uint32_t nx, uint32_t ny, uint32_t *rank);
  * register-resident FFMA loop timed with CUDA events. */
 int pb_peak_fp32(double *tflops);
 
+/* Cell-list build that allocates no device memory.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory themselves (a
+ * host framework that owns all device memory through its own pool, or a
+ * latency-critical loop that must not allocate).  Same result as
+ * pb_md_build_cells, bit for bit, with every scratch array held in one static
+ * device array of fixed size (see pb_cells_build_noalloc_limits): n at most
+ * 131,072 atoms and at most 65,536 cells, larger inputs return PB_ERR_ARG.
+ * Device pointers: r4 (float4[n] positions), type (uint16[n] or NULL for all
+ * zero); outputs start (uint32[C+1], C from pb_plan_grid, cells in the key
+ * order of pb_plan_columns, z fastest), pid (uint32[n]), slot (uint32[n]),
+ * rs4 (float4[n] sorted positions, w = type bits).  Runs on `stream` (a
+ * cudaStream_t, NULL = legacy default) and returns after it has finished.
+ * The first call on a device resolves the static array's device address; make
+ * that first call before any stream capture.  All calls share the one array:
+ * calls that overlap on the GPU race, so serialise them. */
+int pb_cells_build_noalloc(const void *r4, const uint16_t *type, uint32_t n, const float cell6[6],
+                           float rmax, uint32_t *start, uint32_t *pid, uint32_t *slot, void *rs4,
+                           void *stream);
+/* Size limits and static scratch size of pb_cells_build_noalloc. */
+int pb_cells_build_noalloc_limits(uint32_t *max_atoms, uint32_t *max_cells, size_t *scratch_bytes);
+
 /* Library version string. */
 const char *pb_version(void);
 
