@@ -224,6 +224,83 @@ int pb_cells_build_noalloc(const void *r4, const uint16_t *type, uint32_t n, con
 /* Size limits and static scratch size of pb_cells_build_noalloc. */
 int pb_cells_build_noalloc_limits(uint32_t *max_atoms, uint32_t *max_cells, size_t *scratch_bytes);
 
+/* ---- batches of independent systems ----------------------------------------
+ *
+ * No counterpart in the reference, which runs one system per process
+ * (testMD2.cu).  A pb_batch holds many independent periodic LJ systems of
+ * any sizes packed into shared device arrays; one launch per kernel advances
+ * all of them, and whole steps replay from one CUDA graph.  Every system is
+ * computed exactly as a pb_md handle computes it alone (same cell list, same
+ * force and integration arithmetic, per-system FP64 sums in the same order):
+ * its results are bit-identical alone and in any batch.  Systems are
+ * numbered 0 .. nsys-1 in creation order. */
+typedef struct pb_batch pb_batch;
+
+/* natoms[nsys] atoms per system; flags as pb_md_create. */
+int pb_batch_create(const uint32_t *natoms, uint32_t nsys, uint32_t flags, pb_batch **out);
+/* A new batch whose system k continues system src[k] of `old` (state,
+ * box, LJ table, dt, kB and the Gaussian friction carried over bit for bit)
+ * or, when src[k] < 0, is a new system of natoms[k] atoms to be set up with
+ * pb_batch_set_system and pb_batch_import.  natoms[k] is ignored when
+ * src[k] >= 0.  Call pb_batch_setup_cells before stepping. */
+int pb_batch_repack(const pb_batch *old, const int32_t *src, const uint32_t *natoms, uint32_t nsys,
+                    pb_batch **out);
+int pb_batch_destroy(pb_batch *b);
+int pb_batch_set_stream(pb_batch *b, void *stream);
+const char *pb_batch_last_error(const pb_batch *b);
+/* *nsys systems, *natoms_total atoms; atom0 (optional, nsys + 1 entries):
+ * first packed atom of every system. */
+int pb_batch_size(const pb_batch *b, uint32_t *nsys, uint32_t *natoms_total, uint32_t *atom0);
+/* Box, LJ cutoff (rmax2 = rc^2), LJ (sigma, epsilon) per ordered type pair,
+ * time step and kB of system `sys` (setCell, rmax2, setLJparams of one
+ * system). */
+int pb_batch_set_system(pb_batch *b, uint32_t sys, const float cell6[6], float rc,
+                        const float *sigma_eps, uint32_t ntypes, float dt, float kB);
+/* Per-pair cutoffs for system `sys` (pb_md_set_lj_cut): (sigma, epsilon, rc)
+ * per ordered type pair, after pb_batch_set_system. */
+int pb_batch_set_lj_cut(pb_batch *b, uint32_t sys, const float *sigma_eps_rc, uint32_t ntypes);
+/* As pb_md_import_arrays, for system `sys`. */
+int pb_batch_import(pb_batch *b, uint32_t sys, const double *r3, const double *v3,
+                    const double *mass, const uint32_t *type);
+/* Cell grids of all systems; rmax[sys] per system, or NULL for each system's
+ * LJ cutoff. */
+int pb_batch_setup_cells(pb_batch *b, const float *rmax);
+/* Cell build + force for all systems (pb_md_build_cells + pb_md_force). */
+int pb_batch_force(pb_batch *b, uint32_t flags);
+int pb_batch_clear_force(pb_batch *b);
+/* `steps` whole steps of every system (pb_md_run), each with its own dt. */
+int pb_batch_run(pb_batch *b, int mode, uint32_t steps);
+int pb_batch_run_timed(pb_batch *b, int mode, uint32_t steps, float *ms);
+int pb_batch_profile(pb_batch *b, int mode, uint32_t steps, double ms[3]);
+/* Step budgets: system s runs steps[s] more time steps and then stays as it
+ * is while the others go on (its cells are still binned, but no force or
+ * integration work is done for it), so systems with different step counts
+ * share one graph replay and each ends after exactly its own count.  NULL
+ * removes the budgets.  pb_batch_get_steps_left reads the counters back. */
+int pb_batch_set_steps_left(pb_batch *b, const uint32_t *steps);
+int pb_batch_get_steps_left(pb_batch *b, uint32_t *steps);
+/* Per-system sums (out[nsys]), temperatures (T[nsys]), status words
+ * (bits[nsys], cleared by the call). */
+int pb_batch_reduce(pb_batch *b, pb_md_sums *out);
+int pb_batch_temperature(pb_batch *b, double *T);
+int pb_batch_status(pb_batch *b, uint32_t *bits);
+/* Per-system factors / v1 values (nsys doubles each). */
+int pb_batch_scale_velocities(pb_batch *b, const double *s);
+int pb_batch_adjust_velocities(pb_batch *b, const double *v1);
+/* Per-atom fields R, V, VD, F, FOLD, MINV, TYPE, MASS of system `sys`
+ * (sizes as pb_md_get for that system's atom count). */
+int pb_batch_get(pb_batch *b, uint32_t sys, int field, void *host, size_t bytes);
+int pb_batch_set(pb_batch *b, uint32_t sys, int field, const void *host, size_t bytes);
+/* Launch parameters of the force kernel, chosen by the caller or an
+ * autotuner: threads per CTA (128 or 256), and a scale for the z-run length
+ * of every work item (1.0 = default; forces do not depend on either).  Takes
+ * effect at the next pb_batch_setup_cells. */
+int pb_batch_set_tuning(pb_batch *b, int force_threads, float seg_scale);
+/* Bytes of device memory a batch of these systems holds after setup_cells
+ * (estimate from the atom counts and grids; used for admission control). */
+int pb_batch_estimate_bytes(const uint32_t *natoms, const float *cells6, const float *rmax,
+                            uint32_t nsys, uint32_t flags, size_t *bytes);
+
 /* Library version string. */
 const char *pb_version(void);
 

@@ -91,6 +91,31 @@ def _declare(L: C.CDLL) -> None:
         "pb_cells_build_noalloc_limits": [C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_size_t)],
         "pb_plan_grid": [C.POINTER(f32), f32, C.POINTER(u32), C.POINTER(f32)],
         "pb_plan_columns": [u32, u32, C.POINTER(u32)],
+        "pb_batch_create": [vp, u32, u32, C.POINTER(vp)],
+        "pb_batch_repack": [vp, vp, vp, u32, C.POINTER(vp)],
+        "pb_batch_destroy": [vp],
+        "pb_batch_set_stream": [vp, vp],
+        "pb_batch_size": [vp, C.POINTER(u32), C.POINTER(u32), vp],
+        "pb_batch_set_system": [vp, u32, C.POINTER(f32), f32, C.POINTER(f32), u32, f32, f32],
+        "pb_batch_set_lj_cut": [vp, u32, C.POINTER(f32), u32],
+        "pb_batch_import": [vp, u32, vp, vp, vp, vp],
+        "pb_batch_setup_cells": [vp, vp],
+        "pb_batch_force": [vp, u32],
+        "pb_batch_clear_force": [vp],
+        "pb_batch_run": [vp, i32, u32],
+        "pb_batch_run_timed": [vp, i32, u32, C.POINTER(f32)],
+        "pb_batch_profile": [vp, i32, u32, C.POINTER(f64)],
+        "pb_batch_set_steps_left": [vp, vp],
+        "pb_batch_get_steps_left": [vp, vp],
+        "pb_batch_reduce": [vp, vp],
+        "pb_batch_temperature": [vp, vp],
+        "pb_batch_status": [vp, vp],
+        "pb_batch_scale_velocities": [vp, vp],
+        "pb_batch_adjust_velocities": [vp, vp],
+        "pb_batch_get": [vp, u32, i32, vp, C.c_size_t],
+        "pb_batch_set": [vp, u32, i32, vp, C.c_size_t],
+        "pb_batch_set_tuning": [vp, i32, f32],
+        "pb_batch_estimate_bytes": [vp, vp, vp, u32, u32, C.POINTER(C.c_size_t)],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -98,6 +123,8 @@ def _declare(L: C.CDLL) -> None:
         fn.restype = C.c_int
     L.pb_md_last_error.argtypes = [vp]
     L.pb_md_last_error.restype = C.c_char_p
+    L.pb_batch_last_error.argtypes = [vp]
+    L.pb_batch_last_error.restype = C.c_char_p
     L.pb_version.restype = C.c_char_p
 
 
@@ -114,9 +141,10 @@ def lib() -> C.CDLL:
     return _lib
 
 
-def check(code: int, what: str, handle=None) -> None:
+def check(code: int, what: str, handle=None, batch: bool = False) -> None:
     if code != PB_OK:
         detail = ""
         if handle is not None:
-            detail = lib().pb_md_last_error(handle).decode(errors="replace")
+            err = lib().pb_batch_last_error if batch else lib().pb_md_last_error
+            detail = err(handle).decode(errors="replace")
         raise PBError(code, what, detail)

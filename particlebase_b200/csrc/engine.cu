@@ -1,0 +1,662 @@
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+
+#include "../../include/pb/pb.h"
+#include "plan.h"
+
+namespace pb {
+namespace {
+
+int fail(Engine &e, int code, const std::string &msg) {
+  e.err = msg;
+  return code;
+}
+
+int cuda_fail(Engine &e, cudaError_t c, const char *what) {
+  return fail(e, PB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(c));
+}
+
+#define E_CUDA(call)                                       \
+  do {                                                     \
+    cudaError_t c_ = (call);                               \
+    if (c_ != cudaSuccess) return cuda_fail(e, c_, #call); \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t count) {
+  if (count == 0) count = 1;
+  return cudaMalloc((void **)p, sizeof(T) * count);
+}
+
+template <typename T>
+void dfree(T *&p) {
+  if (p) cudaFree((void *)p);
+  p = nullptr;
+}
+
+void free_cells(Engine &e) {
+  dfree(e.key);
+  dfree(e.within);
+  dfree(e.count);
+  dfree(e.start);
+  dfree(e.tilesum);
+  dfree(e.pid_tmp);
+  dfree(e.pid);
+  dfree(e.slot);
+  dfree(e.rs);
+  dfree(e.colrank);
+  dfree(e.colxy);
+  dfree(e.d_sys);
+  dfree(e.d_items);
+  dfree(e.d_item0);
+  dfree(e.fpartials);
+  e.cells_ready = false;
+}
+
+}  // namespace
+
+void engine_drop_graph(Engine &e) {
+  if (e.graph) cudaGraphExecDestroy(e.graph);
+  e.graph = nullptr;
+  e.graph_mode = -1;
+  e.graph_dt.clear();
+}
+
+int engine_init(Engine &e, const uint32_t *natoms, uint32_t nsys, uint32_t flags) {
+  if (!natoms || nsys == 0) return fail(e, PB_ERR_ARG, "no systems");
+  e.flags = flags;
+  e.nsys = nsys;
+  e.sp.assign(nsys, SysParams{});
+  e.atom0.assign(nsys + 1, 0);
+  uint64_t total = 0;
+  for (uint32_t s = 0; s < nsys; ++s) {
+    if (natoms[s] == 0) return fail(e, PB_ERR_ARG, "empty system");
+    e.sp[s].n = natoms[s];
+    e.atom0[s] = (uint32_t)total;
+    total += natoms[s];
+  }
+  if (total >= (1ull << 31)) return fail(e, PB_ERR_ARG, "too many atoms");
+  e.N = (uint32_t)total;
+  e.atom0[nsys] = e.N;
+  E_CUDA(cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking));
+  e.own_stream = true;
+
+  // integration blocks aligned to every system's first atom
+  std::vector<uint32_t> blk0(nsys), nblk(nsys);
+  e.nblocks = 0;
+  for (uint32_t s = 0; s < nsys; ++s) e.nblocks += blocks_for(natoms[s]);
+  std::vector<BlockMap> map(e.nblocks);
+  make_block_map(natoms, nsys, map.data(), blk0.data(), nblk.data());
+  e.sysint.assign(nsys, SysInt{});
+  for (uint32_t s = 0; s < nsys; ++s) {
+    SysInt &I = e.sysint[s];
+    I.atom0 = e.atom0[s];
+    I.natoms = natoms[s];
+    I.vd0 = 3 * e.atom0[s];
+    I.blk0 = blk0[s];
+    I.nblk = nblk[s];
+    I.dt = e.sp[s].dt;
+    for (int k = 0; k < 3; ++k) {
+      I.c0[k] = 0.f;
+      I.c1[k] = 1.f;
+      I.L[k] = 1.f;
+    }
+  }
+  const uint32_t N = e.N;
+  bool ok = dalloc(&e.r, N) == cudaSuccess && dalloc(&e.F[0], N) == cudaSuccess &&
+            dalloc(&e.F[1], N) == cudaSuccess && dalloc(&e.minv, N) == cudaSuccess &&
+            dalloc(&e.mass, N) == cudaSuccess && dalloc(&e.type, N) == cudaSuccess &&
+            dalloc(&e.d_sysint, nsys) == cudaSuccess && dalloc(&e.d_map, e.nblocks) == cudaSuccess &&
+            dalloc(&e.ipartials, (size_t)8 * e.nblocks) == cudaSuccess &&
+            dalloc(&e.sc, nsys) == cudaSuccess && dalloc(&e.status, nsys) == cudaSuccess &&
+            dalloc(&e.d_fac, nsys) == cudaSuccess && dalloc(&e.d_lj, nsys) == cudaSuccess;
+  if (flags & PB_MD_VEL_FP64)
+    ok = ok && dalloc(&e.vd, (size_t)3 * N) == cudaSuccess;
+  else
+    ok = ok && dalloc(&e.v, N) == cudaSuccess;
+  if (nsys > 1) ok = ok && dalloc(&e.sysid, N) == cudaSuccess;
+  if (!ok) return fail(e, PB_ERR_OOM, "device allocation failed");
+  E_CUDA(cudaMemsetAsync(e.r, 0, sizeof(float4) * N, e.stream));
+  E_CUDA(cudaMemsetAsync(e.F[0], 0, sizeof(float4) * N, e.stream));
+  E_CUDA(cudaMemsetAsync(e.F[1], 0, sizeof(float4) * N, e.stream));
+  if (e.v) E_CUDA(cudaMemsetAsync(e.v, 0, sizeof(float4) * N, e.stream));
+  if (e.vd) E_CUDA(cudaMemsetAsync(e.vd, 0, sizeof(double) * 3 * N, e.stream));
+  E_CUDA(cudaMemsetAsync(e.type, 0, sizeof(uint16_t) * N, e.stream));
+  E_CUDA(cudaMemsetAsync(e.sc, 0, sizeof(DevScalars) * nsys, e.stream));
+  E_CUDA(cudaMemsetAsync(e.status, 0, sizeof(uint32_t) * nsys, e.stream));
+  E_CUDA(cudaMemcpyAsync(e.d_map, map.data(), sizeof(BlockMap) * e.nblocks, cudaMemcpyHostToDevice,
+                         e.stream));
+  if (e.sysid) {
+    std::vector<uint32_t> sid(N);
+    for (uint32_t s = 0; s < nsys; ++s)
+      for (uint32_t i = e.atom0[s]; i < e.atom0[s + 1]; ++i) sid[i] = s;
+    E_CUDA(cudaMemcpyAsync(e.sysid, sid.data(), 4 * (size_t)N, cudaMemcpyHostToDevice, e.stream));
+    E_CUDA(cudaStreamSynchronize(e.stream));
+  }
+  if (const char *t = std::getenv("PB_FORCE_THREADS")) e.force_threads = std::atoi(t);
+  int rc = engine_upload_sysint(e);
+  if (rc) return rc;
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  return PB_OK;
+}
+
+void engine_free(Engine &e) {
+  if (e.stream) cudaStreamSynchronize(e.stream);
+  engine_drop_graph(e);
+  free_cells(e);
+  dfree(e.r);
+  dfree(e.v);
+  dfree(e.vd);
+  dfree(e.F[0]);
+  dfree(e.F[1]);
+  dfree(e.minv);
+  dfree(e.mass);
+  dfree(e.type);
+  dfree(e.sysid);
+  dfree(e.d_sysint);
+  dfree(e.d_map);
+  dfree(e.ipartials);
+  dfree(e.sc);
+  dfree(e.status);
+  dfree(e.d_fac);
+  dfree(e.d_lj);
+  dfree(e.steps_left);
+  if (e.own_stream && e.stream) cudaStreamDestroy(e.stream);
+  e.stream = nullptr;
+}
+
+int engine_set_stream(Engine &e, cudaStream_t s) {
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  engine_drop_graph(e);
+  if (e.own_stream) cudaStreamDestroy(e.stream);
+  e.stream = s;
+  e.own_stream = false;
+  return PB_OK;
+}
+
+int engine_upload_lj(Engine &e) {
+  std::vector<LJTable> t(e.nsys);
+  for (uint32_t s = 0; s < e.nsys; ++s) t[s] = e.sp[s].lj;
+  E_CUDA(cudaMemcpyAsync(e.d_lj, t.data(), sizeof(LJTable) * e.nsys, cudaMemcpyHostToDevice,
+                         e.stream));
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  return PB_OK;
+}
+
+int engine_upload_sysint(Engine &e) {
+  for (uint32_t s = 0; s < e.nsys; ++s) {
+    SysInt &I = e.sysint[s];
+    const SysParams &P = e.sp[s];
+    I.dt = P.dt;
+    for (int k = 0; k < 3; ++k) {
+      I.c0[k] = P.cell[2 * k];
+      I.c1[k] = P.cell[2 * k + 1];
+      I.L[k] = P.cell[2 * k + 1] - P.cell[2 * k];
+    }
+  }
+  E_CUDA(cudaMemcpyAsync(e.d_sysint, e.sysint.data(), sizeof(SysInt) * e.nsys,
+                         cudaMemcpyHostToDevice, e.stream));
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  return PB_OK;
+}
+
+void lj_table_fill(SysParams &P, const float *p, uint32_t nt, int stride, bool percut) {
+  LJTable &t = P.lj;
+  std::memset(&t, 0, sizeof(t));
+  t.nt = (int)nt;
+  for (uint32_t a = 0; a < nt; ++a)
+    for (uint32_t b = 0; b < nt; ++b) {
+      const uint32_t k = a * nt + b;
+      const float sig = p[stride * k], eps = p[stride * k + 1];
+      t.s2[k] = sig * sig;
+      t.e24[k] = eps * 24.0f;
+      t.e4[k] = eps * 4.0f;
+      const float rc2 = percut ? p[stride * k + 2] * p[stride * k + 2] : P.rmax2;
+      t.rc2[k] = rc2;
+      const double sr6 = rc2 > 0 ? std::pow((double)t.s2[k] / rc2, 3) : 0.0;
+      t.ushift[k] = (float)(4.0 * eps * (sr6 * sr6 - sr6));
+    }
+  P.lj_set = true;
+  P.lj_percut = percut;
+}
+
+void lj_table_set_rmax2(SysParams &P, float rmax2) {
+  P.rmax2 = rmax2;
+  if (!P.lj_set || P.lj_percut) return;
+  for (int k = 0; k < P.lj.nt * P.lj.nt; ++k) {
+    P.lj.rc2[k] = rmax2;
+    const double sr6 = std::pow((double)P.lj.s2[k] / rmax2, 3);
+    P.lj.ushift[k] = (float)((double)P.lj.e4[k] * (sr6 * sr6 - sr6));
+  }
+}
+
+void engine_set_dt(Engine &e, float dt) {
+  bool changed = false;
+  for (auto &P : e.sp) {
+    if (P.dt != dt) changed = true;
+    P.dt = dt;
+  }
+  if (changed) engine_upload_sysint(e);
+}
+
+int engine_import(Engine &e, uint32_t sys, const double *r3, const double *v3, const double *mass,
+                  const uint32_t *type) {
+  if (sys >= e.nsys || !r3) return fail(e, PB_ERR_ARG, "bad system or positions");
+  const uint32_t n = e.sp[sys].n, a0 = e.atom0[sys];
+  std::vector<float4> r4(n), v4(n, make_float4(0, 0, 0, 0));
+  std::vector<float> minv(n, 1.f), m(n, 1.f);
+  std::vector<uint16_t> t(n, 0);
+  double msum = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    r4[i] = make_float4((float)r3[3 * i], (float)r3[3 * i + 1], (float)r3[3 * i + 2], 0.f);
+    if (v3) v4[i] = make_float4((float)v3[3 * i], (float)v3[3 * i + 1], (float)v3[3 * i + 2], 0.f);
+    const double mi = mass ? mass[i] : 1.0;
+    if (!(mi > 0)) return fail(e, PB_ERR_ARG, "mass must be positive");
+    minv[i] = (float)(1.0 / mi);  // cudaParticleBase::import: TMP[i] = 1.0 / m
+    m[i] = 1.0f / minv[i];        // cudaParticleMD::setM: m = 1 / minv
+    msum += mi;
+    if (type) {
+      if (type[i] >= (uint32_t)kMaxTypes) return fail(e, PB_ERR_ARG, "type id >= 8");
+      t[i] = (uint16_t)type[i];
+    }
+  }
+  e.sp[sys].m0 = msum / n;
+  E_CUDA(cudaMemcpyAsync(e.r + a0, r4.data(), 16 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
+  E_CUDA(cudaMemcpyAsync(e.minv + a0, minv.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
+  E_CUDA(cudaMemcpyAsync(e.mass + a0, m.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
+  E_CUDA(cudaMemcpyAsync(e.type + a0, t.data(), 2 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
+  if (e.vd) {
+    std::vector<double> vd((size_t)3 * n, 0.0);
+    if (v3)
+      for (uint32_t i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) vd[(size_t)k * n + i] = v3[3 * i + k];
+    E_CUDA(cudaMemcpyAsync(e.vd + 3 * (size_t)a0, vd.data(), 24 * (size_t)n,
+                           cudaMemcpyHostToDevice, e.stream));
+    E_CUDA(cudaStreamSynchronize(e.stream));
+  } else {
+    E_CUDA(cudaMemcpyAsync(e.v + a0, v4.data(), 16 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
+    E_CUDA(cudaStreamSynchronize(e.stream));
+  }
+  return PB_OK;
+}
+
+int engine_setup_cells(Engine &e) {
+  free_cells(e);
+  engine_drop_graph(e);
+  std::vector<uint32_t> rank_all, xy_all;
+  std::vector<ForceItem> items;
+  std::vector<SysDesc> sd(e.nsys);
+  e.item0.assign(e.nsys + 1, 0);
+  e.cell0.assign(e.nsys + 1, 0);
+  uint64_t ncells = 0;
+  e.cap_max = 0;
+  for (uint32_t s = 0; s < e.nsys; ++s) {
+    SysParams &P = e.sp[s];
+    if (!P.cell_set) return fail(e, PB_ERR_STATE, "set the cell first");
+    Grid g;
+    if (!make_grid(P.cell, P.rmax, g))
+      return fail(e, PB_ERR_ARG, "cell grid needs at least 3 cells per axis (blocknum > 2)");
+    P.grid = g;
+    const double apc = (double)P.n / g.ncells;
+    P.seg = choose_segment(apc, g.n[2], e.seg_scale);
+    P.cap = (uint32_t)choose_capacity(apc, P.seg);
+    e.cap_max = std::max(e.cap_max, P.cap);
+    std::vector<uint32_t> rank, xy;
+    morton_columns(g.n[0], g.n[1], rank, xy);
+    e.cell0[s] = (uint32_t)ncells;
+    e.item0[s] = (uint32_t)items.size();
+    append_items(s, g, P.seg, (uint32_t)ncells, rank, xy, items);
+    P.key_of_ref.assign(g.ncells, 0);
+    P.ref_of_key.assign(g.ncells, 0);
+    for (int d0 = 0; d0 < g.n[0]; ++d0)
+      for (int d1 = 0; d1 < g.n[1]; ++d1)
+        for (int d2 = 0; d2 < g.n[2]; ++d2) {
+          const uint32_t ref = d2 + d1 * g.n[2] + d0 * g.n[2] * g.n[1];
+          const uint32_t key = rank[d0 * g.n[1] + d1] * g.n[2] + d2;
+          P.key_of_ref[ref] = key;
+          P.ref_of_key[key] = ref;
+        }
+    SysDesc &D = sd[s];
+    D.g = g;
+    D.atom0 = e.atom0[s];
+    D.natoms = P.n;
+    D.cell0 = (uint32_t)ncells;
+    D.col0 = (uint32_t)rank_all.size();
+    D.vd0 = 3 * e.atom0[s];
+    D.lj = s;
+    D.dt = P.dt;
+    D.cap = P.cap;
+    rank_all.insert(rank_all.end(), rank.begin(), rank.end());
+    xy_all.insert(xy_all.end(), xy.begin(), xy.end());
+    ncells += g.ncells;
+    if (ncells >= 0xffffffffull) return fail(e, PB_ERR_ARG, "too many cells");
+  }
+  e.item0[e.nsys] = (uint32_t)items.size();
+  e.cell0[e.nsys] = (uint32_t)ncells;
+  e.ncells = (uint32_t)ncells;
+  e.nitems = (uint32_t)items.size();
+  const uint32_t N = e.N, C = e.ncells;
+  const uint32_t ntiles = (C + 4095) / 4096;
+  bool ok = dalloc(&e.key, N) == cudaSuccess && dalloc(&e.within, N) == cudaSuccess &&
+            dalloc(&e.count, C) == cudaSuccess && dalloc(&e.start, (size_t)C + 1) == cudaSuccess &&
+            dalloc(&e.tilesum, ntiles) == cudaSuccess && dalloc(&e.pid_tmp, N) == cudaSuccess &&
+            dalloc(&e.pid, N) == cudaSuccess && dalloc(&e.slot, N) == cudaSuccess &&
+            dalloc(&e.rs, N) == cudaSuccess && dalloc(&e.colrank, rank_all.size()) == cudaSuccess &&
+            dalloc(&e.colxy, xy_all.size()) == cudaSuccess &&
+            dalloc(&e.d_sys, e.nsys) == cudaSuccess && dalloc(&e.d_items, items.size()) == cudaSuccess &&
+            dalloc(&e.d_item0, e.nsys + 1) == cudaSuccess &&
+            dalloc(&e.fpartials, (size_t)4 * items.size()) == cudaSuccess;
+  if (!ok) {
+    free_cells(e);
+    return fail(e, PB_ERR_OOM, "cell list allocation failed");
+  }
+  E_CUDA(cudaMemsetAsync(e.count, 0, sizeof(uint32_t) * C, e.stream));
+  E_CUDA(cudaMemcpyAsync(e.colrank, rank_all.data(), 4 * rank_all.size(), cudaMemcpyHostToDevice,
+                         e.stream));
+  E_CUDA(cudaMemcpyAsync(e.colxy, xy_all.data(), 4 * xy_all.size(), cudaMemcpyHostToDevice,
+                         e.stream));
+  E_CUDA(cudaMemcpyAsync(e.d_sys, sd.data(), sizeof(SysDesc) * e.nsys, cudaMemcpyHostToDevice,
+                         e.stream));
+  E_CUDA(cudaMemcpyAsync(e.d_items, items.data(), sizeof(ForceItem) * items.size(),
+                         cudaMemcpyHostToDevice, e.stream));
+  E_CUDA(cudaMemcpyAsync(e.d_item0, e.item0.data(), 4 * (size_t)(e.nsys + 1),
+                         cudaMemcpyHostToDevice, e.stream));
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  int rc = engine_upload_sysint(e);
+  if (rc) return rc;
+  e.cells_ready = true;
+  return PB_OK;
+}
+
+bool engine_ready(const Engine &e) {
+  if (!e.cells_ready || e.N == 0) return false;
+  for (const auto &P : e.sp)
+    if (!P.lj_set) return false;
+  return true;
+}
+
+IntegrateArgs engine_iargs(Engine &e, int wrap) {
+  IntegrateArgs a{};
+  a.r = e.r;
+  a.v = e.vd ? nullptr : e.v;
+  a.vd = e.vd;
+  a.F = e.F[e.cur];
+  a.Fold = e.F[1 - e.cur];
+  a.minv = e.minv;
+  a.mass = e.mass;
+  a.sys = e.d_sysint;
+  a.map = e.d_map;
+  a.nblocks = e.nblocks;
+  a.wrap = wrap;
+  a.sc = e.sc;
+  a.partials = e.ipartials;
+  a.status = e.status;
+  a.steps_left = e.steps_left;
+  return a;
+}
+
+CellBufs engine_cbufs(Engine &e) {
+  CellBufs b{};
+  b.r = e.r;
+  b.type = e.type;
+  b.sysid = e.nsys > 1 ? e.sysid : nullptr;
+  b.sys = e.d_sys;
+  b.colrank = e.colrank;
+  b.N = e.N;
+  b.ncells = e.ncells;
+  b.key = e.key;
+  b.within = e.within;
+  b.count = e.count;
+  b.start = e.start;
+  b.tilesum = e.tilesum;
+  b.pid_tmp = e.pid_tmp;
+  b.pid = e.pid;
+  b.slot = e.slot;
+  b.rs = e.rs;
+  b.status = e.status;
+  return b;
+}
+
+ForceBufs engine_fbufs(Engine &e) {
+  ForceBufs b{};
+  b.rs = e.rs;
+  b.start = e.start;
+  b.pid = e.pid;
+  b.sys = e.d_sys;
+  b.colxy = e.colxy;
+  b.colrank = e.colrank;
+  b.lj = e.d_lj;
+  b.items = e.d_items;
+  b.nitems = e.nitems;
+  b.cap = (int)e.cap_max;
+  b.F = e.F[e.cur];
+  b.partials = e.fpartials;
+  b.status = e.status;
+  b.steps_left = e.steps_left;
+  return b;
+}
+
+int engine_build(Engine &e) {
+  if (!e.cells_ready) return fail(e, PB_ERR_STATE, "setup_cells first");
+  cudaError_t c = launch_cell_build(engine_cbufs(e), e.stream);
+  if (c != cudaSuccess) return cuda_fail(e, c, "cell build");
+  return PB_OK;
+}
+
+int engine_force(Engine &e, bool energy) {
+  if (!engine_ready(e)) return fail(e, PB_ERR_STATE, "need cell, LJ parameters and setup_cells");
+  int nt = 1;
+  for (const auto &P : e.sp) nt = std::max(nt, P.lj.nt);
+  cudaError_t c = launch_force(engine_fbufs(e), nt, energy, (e.flags & PB_MD_ACC_FP64) != 0,
+                               e.force_threads, e.stream);
+  if (c != cudaSuccess) return cuda_fail(e, c, "force");
+  e.last = e.cur;
+  if (energy) {
+    c = launch_energy_total(e.fpartials, e.d_item0, e.nsys, e.sc, e.stream);
+    if (c != cudaSuccess) return cuda_fail(e, c, "energy total");
+  }
+  e.energy_valid = energy;
+  return PB_OK;
+}
+
+int engine_evolve(Engine &e, int mode, int wrap) {
+  IntegrateArgs a = engine_iargs(e, wrap);
+  cudaError_t c;
+  if (mode == PB_MODE_VV) {
+    if (e.vd) return fail(e, PB_ERR_UNSUPPORTED, "velocity Verlet uses FP32 velocities");
+    c = launch_vv(a, e.stream);
+  } else {
+    c = launch_gauss(a, e.stream);
+  }
+  if (c != cudaSuccess) return cuda_fail(e, c, "time evolution");
+  e.cur = 1 - e.cur;
+  ++e.steps_done;
+  return PB_OK;
+}
+
+int engine_wrap(Engine &e) {
+  cudaError_t c = launch_wrap(engine_iargs(e, 1), e.stream);
+  if (c != cudaSuccess) return cuda_fail(e, c, "wrap");
+  return PB_OK;
+}
+
+int engine_step(Engine &e, int mode) {
+  int rc = engine_build(e);
+  if (!rc) rc = engine_force(e, false);
+  if (!rc) rc = engine_evolve(e, mode, 1);
+  return rc;
+}
+
+int engine_run(Engine &e, int mode, uint32_t steps) {
+  if (!engine_ready(e)) return fail(e, PB_ERR_STATE, "need cell, LJ parameters and setup_cells");
+  if (mode != PB_MODE_VV && mode != PB_MODE_GAUSS) return fail(e, PB_ERR_ARG, "bad mode");
+  if (mode == PB_MODE_VV && e.vd) return fail(e, PB_ERR_UNSUPPORTED, "VV needs FP32 velocities");
+  std::vector<float> dts(e.nsys);
+  for (uint32_t s = 0; s < e.nsys; ++s) dts[s] = e.sp[s].dt;
+  uint32_t done = 0;
+  if (steps >= 2) {
+    if (!e.graph || e.graph_mode != mode || e.graph_dt != dts) {
+      engine_drop_graph(e);
+      cudaGraph_t g = nullptr;
+      const int cur0 = e.cur, last0 = e.last;
+      const uint64_t done0 = e.steps_done;
+      E_CUDA(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
+      int rc = engine_step(e, mode);
+      if (!rc) rc = engine_step(e, mode);
+      cudaError_t c = cudaStreamEndCapture(e.stream, &g);
+      e.cur = cur0;  // the captured steps have not run yet
+      e.last = last0;
+      e.steps_done = done0;
+      if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (c != cudaSuccess) return cuda_fail(e, c, "graph capture");
+      c = cudaGraphInstantiate(&e.graph, g, 0);
+      cudaGraphDestroy(g);
+      if (c != cudaSuccess) {
+        e.graph = nullptr;
+        return cuda_fail(e, c, "graph instantiate");
+      }
+      e.graph_mode = mode;
+      e.graph_dt = dts;
+    }
+    for (; done + 2 <= steps; done += 2) {
+      E_CUDA(cudaGraphLaunch(e.graph, e.stream));
+      e.steps_done += 2;
+      e.last = 1 - e.cur;  // two steps: cur is back where it was, F[1 - cur] is the newest
+    }
+  }
+  for (; done < steps; ++done) {
+    int rc = engine_step(e, mode);
+    if (rc) return rc;
+  }
+  e.energy_valid = false;
+  return PB_OK;
+}
+
+int engine_profile(Engine &e, int mode, uint32_t steps, double ms[3]) {
+  if (!engine_ready(e) || steps == 0) return fail(e, PB_ERR_STATE, "not ready");
+  cudaEvent_t ev[4];
+  for (auto &x : ev) E_CUDA(cudaEventCreate(&x));
+  double acc[3] = {0, 0, 0};
+  int rc = PB_OK;
+  for (uint32_t k = 0; k < steps && !rc; ++k) {
+    cudaEventRecord(ev[0], e.stream);
+    rc = engine_build(e);
+    cudaEventRecord(ev[1], e.stream);
+    if (!rc) rc = engine_force(e, false);
+    cudaEventRecord(ev[2], e.stream);
+    if (!rc) rc = engine_evolve(e, mode, 1);
+    cudaEventRecord(ev[3], e.stream);
+    cudaEventSynchronize(ev[3]);
+    for (int p = 0; p < 3; ++p) {
+      float t = 0;
+      cudaEventElapsedTime(&t, ev[p], ev[p + 1]);
+      acc[p] += t;
+    }
+  }
+  for (auto &x : ev) cudaEventDestroy(x);
+  for (int p = 0; p < 3; ++p) ms[p] = acc[p] / steps;
+  return rc;
+}
+
+int engine_set_steps_left(Engine &e, const uint32_t *steps) {
+  if (!steps) {
+    if (e.steps_left) {
+      E_CUDA(cudaStreamSynchronize(e.stream));
+      dfree(e.steps_left);
+      engine_drop_graph(e);  // captured launches hold the old pointer
+    }
+    return PB_OK;
+  }
+  if (!e.steps_left) {
+    if (dalloc(&e.steps_left, e.nsys) != cudaSuccess) return fail(e, PB_ERR_OOM, "steps_left");
+    engine_drop_graph(e);  // captured launches hold the old (null) pointer
+  }
+  e.budget_set.assign(e.nsys, e.steps_done);
+  e.budget_end.resize(e.nsys);
+  e.last_at_set.assign(e.nsys, e.last);
+  for (uint32_t s = 0; s < e.nsys; ++s) e.budget_end[s] = e.steps_done + steps[s];
+  E_CUDA(cudaMemcpyAsync(e.steps_left, steps, 4 * (size_t)e.nsys, cudaMemcpyHostToDevice, e.stream));
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  return PB_OK;
+}
+
+int engine_get_steps_left(Engine &e, uint32_t *steps) {
+  if (!e.steps_left) return fail(e, PB_ERR_STATE, "no step budgets set");
+  E_CUDA(cudaMemcpyAsync(steps, e.steps_left, 4 * (size_t)e.nsys, cudaMemcpyDeviceToHost, e.stream));
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  return PB_OK;
+}
+
+bool engine_finished(const Engine &e, uint32_t s) {
+  return e.steps_left && s < e.budget_end.size() && e.steps_done >= e.budget_end[s];
+}
+
+int engine_force_buffer(const Engine &e, uint32_t s) {
+  if (!engine_finished(e, s)) return e.last;
+  if (e.budget_end[s] == e.budget_set[s]) return e.last_at_set[s];  // never ran under this budget
+  // its last step was step j = budget_end - 1; step j's force went to the buffer
+  // that was `cur` then, and cur flips every step
+  const uint64_t back = e.steps_done - (e.budget_end[s] - 1);
+  return (back & 1) ? 1 - e.cur : e.cur;
+}
+
+int engine_clear_force(Engine &e) {
+  E_CUDA(cudaMemsetAsync(e.F[0], 0, sizeof(float4) * e.N, e.stream));
+  E_CUDA(cudaMemsetAsync(e.F[1], 0, sizeof(float4) * e.N, e.stream));
+  return PB_OK;
+}
+
+int engine_mv2(Engine &e) {
+  cudaError_t c = launch_mv2(engine_iargs(e, 0), e.stream);
+  if (c != cudaSuccess) return cuda_fail(e, c, "mv2");
+  return PB_OK;
+}
+
+int engine_fv(Engine &e) {
+  cudaError_t c = launch_fv(engine_iargs(e, 0), e.stream);
+  if (c != cudaSuccess) return cuda_fail(e, c, "fv");
+  return PB_OK;
+}
+
+int engine_scale(Engine &e, const double *factors) {
+  E_CUDA(cudaMemcpyAsync(e.d_fac, factors, sizeof(double) * e.nsys, cudaMemcpyHostToDevice,
+                         e.stream));
+  cudaError_t c = launch_scale(engine_iargs(e, 0), e.d_fac, e.stream);
+  if (c != cudaSuccess) return cuda_fail(e, c, "scale");
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  return PB_OK;
+}
+
+int engine_adjust(Engine &e, const double *v1) {
+  E_CUDA(cudaMemcpyAsync(e.d_fac, v1, sizeof(double) * e.nsys, cudaMemcpyHostToDevice, e.stream));
+  cudaError_t c = launch_adjust(engine_iargs(e, 0), e.d_fac, e.stream);
+  if (c != cudaSuccess) return cuda_fail(e, c, "adjust");
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  return PB_OK;
+}
+
+int engine_scalars(Engine &e, std::vector<DevScalars> &out) {
+  out.resize(e.nsys);
+  E_CUDA(cudaMemcpyAsync(out.data(), e.sc, sizeof(DevScalars) * e.nsys, cudaMemcpyDeviceToHost,
+                         e.stream));
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  return PB_OK;
+}
+
+int engine_status(Engine &e, std::vector<uint32_t> &bits) {
+  bits.resize(e.nsys);
+  E_CUDA(cudaMemcpyAsync(bits.data(), e.status, 4 * (size_t)e.nsys, cudaMemcpyDeviceToHost,
+                         e.stream));
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  E_CUDA(cudaMemsetAsync(e.status, 0, 4 * (size_t)e.nsys, e.stream));
+  return PB_OK;
+}
+
+}  // namespace pb

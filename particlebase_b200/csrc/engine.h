@@ -1,0 +1,137 @@
+// Host engine shared by the single-system handle (pb_md, one system) and the
+// batch handle (pb_batch, many packed systems): device buffers, the cell
+// plan, kernel launch sequences and CUDA-graph replay of whole steps.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "integrate.cuh"
+#include "md.cuh"
+
+namespace pb {
+
+// Host-side parameters of one system.
+struct SysParams {
+  uint32_t n = 0;
+  float cell[6] = {0, 1, 0, 1, 0, 1};
+  bool cell_set = false;
+  float rmax = 0.f, rmax2 = 0.f, kB = 1.f;
+  LJTable lj{};
+  bool lj_set = false, lj_percut = false;
+  Grid grid{};
+  int seg = 1;
+  uint32_t cap = 0;
+  double m0 = 1.0;
+  float dt = 0.005f;
+  std::vector<uint32_t> key_of_ref, ref_of_key;  // reference cell id <-> packed key - cell0
+};
+
+struct Engine {
+  std::string err;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  uint32_t flags = 0;  // PB_MD_VEL_FP64 | PB_MD_ACC_FP64
+  uint32_t nsys = 0, N = 0;
+  std::vector<SysParams> sp;
+  std::vector<uint32_t> atom0;  // first atom of each system (+ total)
+  std::vector<SysInt> sysint;   // host mirror of d_sysint
+  int force_threads = 256;
+  float seg_scale = 1.f;  // z-run length scale of the force work items
+
+  // per-atom state
+  float4 *r = nullptr, *v = nullptr, *F[2] = {nullptr, nullptr};
+  int cur = 0;   // the next force call writes F[cur]; the next step uses F[1 - cur] as Fold
+  int last = 0;  // F[last] holds the most recent force (reference field F)
+  double *vd = nullptr;
+  float *minv = nullptr, *mass = nullptr;
+  uint16_t *type = nullptr;
+  uint32_t *sysid = nullptr;  // only with nsys > 1
+
+  // integration
+  SysInt *d_sysint = nullptr;
+  BlockMap *d_map = nullptr;
+  uint32_t nblocks = 0;
+  double *ipartials = nullptr;
+  DevScalars *sc = nullptr;
+  uint32_t *status = nullptr;
+  double *d_fac = nullptr;  // per-system factors for scale / adjust
+  LJTable *d_lj = nullptr;
+
+  // cell list (after setup_cells)
+  bool cells_ready = false;
+  uint32_t ncells = 0;
+  uint32_t *key = nullptr, *within = nullptr, *count = nullptr, *start = nullptr,
+           *tilesum = nullptr, *pid_tmp = nullptr, *pid = nullptr, *slot = nullptr,
+           *colrank = nullptr, *colxy = nullptr, *d_item0 = nullptr;
+  float4 *rs = nullptr;
+  SysDesc *d_sys = nullptr;
+  ForceItem *d_items = nullptr;
+  uint32_t nitems = 0;
+  std::vector<uint32_t> item0, cell0;
+  double *fpartials = nullptr;
+  uint32_t cap_max = 0;
+  bool energy_valid = false;
+
+  // per-system step budgets (serving): device counters, nullptr = no limits
+  uint32_t *steps_left = nullptr;
+  uint64_t steps_done = 0;           // time steps issued since creation
+  std::vector<uint64_t> budget_set;  // steps_done when each budget was set
+  std::vector<uint64_t> budget_end;  // steps_done at which each budget runs out
+  std::vector<int> last_at_set;      // `last` when each budget was set
+
+  // CUDA graph of two whole steps (the F ping-pong returns to its parity)
+  cudaGraphExec_t graph = nullptr;
+  int graph_mode = -1;
+  std::vector<float> graph_dt;
+};
+
+// All return pb_status codes; on failure e.err says why.
+int engine_init(Engine &e, const uint32_t *natoms, uint32_t nsys, uint32_t flags);
+void engine_free(Engine &e);
+int engine_set_stream(Engine &e, cudaStream_t s);
+int engine_upload_lj(Engine &e);
+int engine_upload_sysint(Engine &e);
+int engine_import(Engine &e, uint32_t sys, const double *r3, const double *v3, const double *mass,
+                  const uint32_t *type);
+int engine_setup_cells(Engine &e);
+bool engine_ready(const Engine &e);
+
+int engine_build(Engine &e);
+int engine_force(Engine &e, bool energy);
+int engine_evolve(Engine &e, int mode, int wrap);
+int engine_wrap(Engine &e);
+int engine_step(Engine &e, int mode);
+int engine_run(Engine &e, int mode, uint32_t steps);
+int engine_profile(Engine &e, int mode, uint32_t steps, double ms[3]);
+int engine_clear_force(Engine &e);
+int engine_mv2(Engine &e);
+int engine_fv(Engine &e);
+int engine_scale(Engine &e, const double *factors);
+int engine_adjust(Engine &e, const double *v1);
+int engine_scalars(Engine &e, std::vector<DevScalars> &out);
+int engine_status(Engine &e, std::vector<uint32_t> &bits);
+void engine_drop_graph(Engine &e);
+void engine_set_dt(Engine &e, float dt);
+// Step budgets: system s runs steps[s] more steps, then its state stays as it
+// is (the force and integration kernels skip it).  steps == nullptr removes
+// all limits.
+int engine_set_steps_left(Engine &e, const uint32_t *steps);
+int engine_get_steps_left(Engine &e, uint32_t *steps);
+// Index of the force buffer holding system s's most recent force.
+int engine_force_buffer(const Engine &e, uint32_t s);
+// True once system s has used up its step budget.
+bool engine_finished(const Engine &e, uint32_t s);
+
+// LJ table of one system from (sigma, epsilon[, rc]) per ordered type pair
+// (stride 2 or 3), as _setLJparams (kernelinline.hh:120-134) stores it:
+// sigma^2 and 24 epsilon, plus the shift of the potential at the cutoff.
+void lj_table_fill(SysParams &P, const float *p, uint32_t nt, int stride, bool percut);
+// Common cutoff rmax2 for a table filled without per-pair cutoffs.
+void lj_table_set_rmax2(SysParams &P, float rmax2);
+
+IntegrateArgs engine_iargs(Engine &e, int wrap);
+CellBufs engine_cbufs(Engine &e);
+ForceBufs engine_fbufs(Engine &e);
+
+}  // namespace pb

@@ -162,6 +162,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_force(ForceBufs b) {
   __shared__ double red[4 * 32];
 
   const ForceItem it = b.items[blockIdx.x];
+  if (b.steps_left != nullptr && b.steps_left[it.sys] == 0) {
+    // a system whose step budget is spent keeps its state; nothing to compute
+    if (ENERGY && threadIdx.x < 4) b.partials[(size_t)blockIdx.x * 4 + threadIdx.x] = 0.0;
+    return;
+  }
   const SysDesc &S = b.sys[it.sys];
   const Grid g = S.g;
   const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
@@ -226,7 +231,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_force(ForceBufs b) {
     }
     if (threadIdx.x == 0) {
       st.total = run;
-      st.overflow = run > (uint32_t)b.cap;
+      st.overflow = run > S.cap;  // the system's own capacity: same path alone or batched
       st.home_g0 = gstart[4][1];
       bool sh = st.sz_lo != 0.f || st.sz_mid != 0.f || st.sz_hi != 0.f;
       for (int c = 0; c < 9; ++c) sh = sh || st.sx[c] != 0.f || st.sy[c] != 0.f;
@@ -257,7 +262,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_force(ForceBufs b) {
     }
     const bool ok = mbar_wait_bounded(&st.bar, 0);
     if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) atomicOr(b.status, kStatusWaitTimeout);
+      // give the copies in flight a second bounded wait before the CTA leaves
+      if (threadIdx.x == 0) atomicOr(&b.status[it.sys], kStatusWaitTimeout);
+      mbar_wait_bounded(&st.bar, 0);
       return;
     }
     if (st.shifted) {
@@ -276,7 +283,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_force(ForceBufs b) {
       __syncthreads();
     }
   } else if (overflow && threadIdx.x == 0) {
-    atomicOr(b.status, kStatusSmemOverflow);
+    atomicOr(&b.status[it.sys], kStatusSmemOverflow);
   }
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

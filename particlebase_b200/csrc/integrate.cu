@@ -1,5 +1,5 @@
 // Velocity Verlet, Gaussian isokinetic thermostat, periodic wrap and the
-// FP64 reductions around them, for one system in particle order.
+// FP64 reductions around them, for one or many packed systems.
 //
 //   k_vv        propagateVelocityVerlet_F4 (kernelfuncs.cu:333-367) fused with
 //               applyPeriodicCondition_F4 (kernelfuncs.cu:87-139) and the
@@ -30,25 +30,94 @@
 namespace pb {
 namespace {
 
-constexpr int kThreads = 256;
-
-__device__ __forceinline__ float4 load_v(const IntegrateArgs &a, uint32_t i) {
-  if (a.vd) return make_float4((float)a.vd[i], (float)a.vd[i + a.N], (float)a.vd[i + 2 * a.N], 0.f);
-  return a.v[i];
+// Per-system "last block finishes the sum": block b (block k of system s,
+// whose blocks are blk0 .. blk0 + nblk - 1) writes its NV partials; the
+// system's last block adds the system's partials in block order.  Returns
+// true in thread 0 of that block, with the totals in `tot`.
+template <int NV>
+__device__ __forceinline__ bool sys_total(const double (&mine)[NV], double *partials, uint32_t b,
+                                          uint32_t blk0, uint32_t nblk, unsigned int *counter,
+                                          double (&tot)[NV], double *scratch) {
+  __shared__ bool is_last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) partials[(size_t)b * NV + k] = mine[k];
+    __threadfence();
+    const unsigned int ticket = atomicAdd(counter, 1u);
+    is_last = (ticket == nblk - 1);
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  __threadfence();
+  double acc[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+  for (uint32_t q = threadIdx.x; q < nblk; q += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] += __ldcg(&partials[(size_t)(blk0 + q) * NV + k]);
+  }
+  block_sum<NV>(acc, scratch);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) tot[k] = acc[k];
+    *counter = 0;
+  }
+  return threadIdx.x == 0;
 }
 
-__device__ __forceinline__ void wrap3(const IntegrateArgs &a, float4 &p) {
-  p.x = wrap_coord(p.x, a.c0[0], a.c1[0], a.L[0]);
-  p.y = wrap_coord(p.y, a.c0[1], a.c1[1], a.L[1]);
-  p.z = wrap_coord(p.z, a.c0[2], a.c1[2], a.L[2]);
+__device__ __forceinline__ bool finished(const IntegrateArgs &a, uint32_t sys) {
+  return a.steps_left != nullptr && a.steps_left[sys] == 0u;
 }
 
-__global__ void __launch_bounds__(kThreads) k_vv(IntegrateArgs a) {
+__device__ __forceinline__ void count_step(const IntegrateArgs &a, uint32_t sys) {
+  if (a.steps_left != nullptr) a.steps_left[sys] -= 1u;
+}
+
+__device__ __forceinline__ void wrap3(const SysInt &S, float4 &p) {
+  p.x = wrap_coord(p.x, S.c0[0], S.c1[0], S.L[0]);
+  p.y = wrap_coord(p.y, S.c0[1], S.c1[1], S.L[1]);
+  p.z = wrap_coord(p.z, S.c0[2], S.c1[2], S.L[2]);
+}
+
+// FP64 velocity of atom i (global index) of system S: plane k at vd0 + k * natoms.
+__device__ __forceinline__ void load_vd(const IntegrateArgs &a, const SysInt &S, uint32_t i,
+                                        double v[3]) {
+  const size_t o = (size_t)S.vd0 + (i - S.atom0);
+  v[0] = a.vd[o];
+  v[1] = a.vd[o + S.natoms];
+  v[2] = a.vd[o + 2 * (size_t)S.natoms];
+}
+
+__device__ __forceinline__ void store_vd(const IntegrateArgs &a, const SysInt &S, uint32_t i,
+                                         const double v[3]) {
+  const size_t o = (size_t)S.vd0 + (i - S.atom0);
+  a.vd[o] = v[0];
+  a.vd[o + S.natoms] = v[1];
+  a.vd[o + 2 * (size_t)S.natoms] = v[2];
+}
+
+__device__ __forceinline__ void load_v(const IntegrateArgs &a, const SysInt &S, uint32_t i,
+                                       double v[3]) {
+  if (a.vd) {
+    load_vd(a, S, i, v);
+  } else {
+    const float4 w = a.v[i];
+    v[0] = w.x;
+    v[1] = w.y;
+    v[2] = w.z;
+  }
+}
+
+__global__ void __launch_bounds__(kIntThreads) k_vv(IntegrateArgs a) {
   __shared__ double red[32];
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const BlockMap m = a.map[blockIdx.x];
+  if (finished(a, m.sys)) return;
+  const SysInt &S = a.sys[m.sys];
   double mv2 = 0;
-  if (i < a.N) {
-    const float dt2 = a.dt * 0.5f;
+  if (threadIdx.x < m.n) {
+    const uint32_t i = m.i0 + threadIdx.x;
+    const float dt = S.dt;
+    const float dt2 = dt * 0.5f;
     const float h = dt2 * a.minv[i];  // dt / 2m
     const float4 F = a.F[i], Fo = a.Fold[i];
     float4 v = a.v[i];
@@ -56,87 +125,86 @@ __global__ void __launch_bounds__(kThreads) k_vv(IntegrateArgs a) {
     v.y += (F.y + Fo.y) * h;
     v.z += (F.z + Fo.z) * h;
     v.w = 0.f;
-    const float h2 = h * a.dt;
+    const float h2 = h * dt;
     float4 p = a.r[i];
-    p.x += v.x * a.dt + F.x * h2;
-    p.y += v.y * a.dt + F.y * h2;
-    p.z += v.z * a.dt + F.z * h2;
-    if (a.wrap) wrap3(a, p);
+    p.x += v.x * dt + F.x * h2;
+    p.y += v.y * dt + F.y * h2;
+    p.z += v.z * dt + F.z * h2;
+    if (a.wrap) wrap3(S, p);
     a.v[i] = v;
     a.r[i] = p;
-    mv2 = (double)a.mass[i] *
-          ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+    mv2 = (double)a.mass[i] * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
   }
-  double m[1] = {mv2}, tot[1];
-  block_sum<1>(m, red);
-  if (last_block_total<1>(m, a.partials, &a.sc->counter[0], tot, red)) {
-    a.sc->mv2 = tot[0];
-    if (!isfinite(tot[0])) atomicOr(a.status, kStatusNonFinite);
+  double s[1] = {mv2}, tot[1];
+  block_sum<1>(s, red);
+  if (sys_total<1>(s, a.partials, blockIdx.x, S.blk0, S.nblk, &a.sc[m.sys].counter[0], tot, red)) {
+    a.sc[m.sys].mv2 = tot[0];
+    if (!isfinite(tot[0])) atomicOr(&a.status[m.sys], kStatusNonFinite);
+    count_step(a, m.sys);  // every block of the system has read steps_left
   }
 }
 
 // A for atom i (FP64), identical arithmetic in both Gaussian passes.
-__device__ __forceinline__ void gauss_A(const IntegrateArgs &a, uint32_t i, double xi_old,
-                                        double A[3], float4 &F) {
-  const float h = (a.dt * 0.5f) * a.minv[i];
+__device__ __forceinline__ void gauss_A(const IntegrateArgs &a, const SysInt &S, uint32_t i,
+                                        double xi_old, double A[3], float4 &F) {
+  const float h = (S.dt * 0.5f) * a.minv[i];
   F = a.F[i];
   const float4 Fo = a.Fold[i];
   double v0[3];
-  if (a.vd) {
-    v0[0] = a.vd[i];
-    v0[1] = a.vd[i + a.N];
-    v0[2] = a.vd[i + 2 * a.N];
-  } else {
-    const float4 v = a.v[i];
-    v0[0] = v.x;
-    v0[1] = v.y;
-    v0[2] = v.z;
-  }
-  const double hx = (double)a.dt * 0.5 * xi_old;
+  load_v(a, S, i, v0);
+  const double hx = (double)S.dt * 0.5 * xi_old;
   A[0] = v0[0] + (double)(F.x + Fo.x) * h - v0[0] * hx;
   A[1] = v0[1] + (double)(F.y + Fo.y) * h - v0[1] * hx;
   A[2] = v0[2] + (double)(F.z + Fo.z) * h - v0[2] * hx;
 }
 
-__global__ void __launch_bounds__(kThreads) k_gauss_a(IntegrateArgs a) {
+__global__ void __launch_bounds__(kIntThreads) k_gauss_a(IntegrateArgs a) {
   __shared__ double red[2 * 32];
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  const double xi_old = a.sc->xi_old;
+  const BlockMap m = a.map[blockIdx.x];
+  if (finished(a, m.sys)) return;
+  const SysInt &S = a.sys[m.sys];
+  DevScalars &sc = a.sc[m.sys];
+  const double xi_old = sc.xi_old;
   double s[2] = {0, 0};
-  if (i < a.N) {
+  if (threadIdx.x < m.n) {
+    const uint32_t i = m.i0 + threadIdx.x;
     double A[3];
     float4 F;
-    gauss_A(a, i, xi_old, A, F);
+    gauss_A(a, S, i, xi_old, A, F);
     s[0] = (double)F.x * A[0] + (double)F.y * A[1] + (double)F.z * A[2];
     s[1] = (double)a.mass[i] * (A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
   }
   double tot[2];
   block_sum<2>(s, red);
-  if (last_block_total<2>(s, a.partials, &a.sc->counter[1], tot, red)) {
-    const double hdt = 0.5 * (double)a.dt;
+  if (sys_total<2>(s, a.partials, blockIdx.x, S.blk0, S.nblk, &sc.counter[1], tot, red)) {
+    const double hdt = 0.5 * (double)S.dt;
     const double c = tot[1] > 0 ? tot[0] / tot[1] : 0.0;
     double xi = (xi_old == 0.0) ? c : c / (1.0 - c * hdt);
     if (!isfinite(xi) || !isfinite(tot[0]) || !isfinite(tot[1])) {
-      atomicOr(a.status, kStatusNonFinite | kStatusNoConverge);
+      atomicOr(&a.status[m.sys], kStatusNonFinite | kStatusNoConverge);
       xi = 0.0;
     }
-    a.sc->sum_fa = tot[0];
-    a.sc->sum_ma2 = tot[1];
-    a.sc->xi_new = xi;
+    sc.sum_fa = tot[0];
+    sc.sum_ma2 = tot[1];
+    sc.xi_new = xi;
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_gauss_b(IntegrateArgs a) {
+__global__ void __launch_bounds__(kIntThreads) k_gauss_b(IntegrateArgs a) {
   __shared__ double red[32];
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  const double xi_old = a.sc->xi_old;
-  const double xi = a.sc->xi_new;
+  const BlockMap m = a.map[blockIdx.x];
+  if (finished(a, m.sys)) return;
+  const SysInt &S = a.sys[m.sys];
+  DevScalars &sc = a.sc[m.sys];
+  const double xi_old = sc.xi_old;
+  const double xi = sc.xi_new;
   double mv2 = 0;
-  if (i < a.N) {
+  if (threadIdx.x < m.n) {
+    const uint32_t i = m.i0 + threadIdx.x;
     double A[3];
     float4 F;
-    gauss_A(a, i, xi_old, A, F);
-    const double dt = a.dt;
+    gauss_A(a, S, i, xi_old, A, F);
+    const double dt = S.dt;
     const double inv = (xi_old == 0.0) ? 1.0 : 1.0 / (1.0 + xi * 0.5 * dt);
     const double v[3] = {A[0] * inv, A[1] * inv, A[2] * inv};
     const double cv = dt - xi * 0.5 * dt * dt;
@@ -145,12 +213,10 @@ __global__ void __launch_bounds__(kThreads) k_gauss_b(IntegrateArgs a) {
     p.x = (float)((double)p.x + v[0] * cv + (double)F.x * cf);
     p.y = (float)((double)p.y + v[1] * cv + (double)F.y * cf);
     p.z = (float)((double)p.z + v[2] * cv + (double)F.z * cf);
-    if (a.wrap) wrap3(a, p);
+    if (a.wrap) wrap3(S, p);
     a.r[i] = p;
     if (a.vd) {
-      a.vd[i] = v[0];
-      a.vd[i + a.N] = v[1];
-      a.vd[i + 2 * a.N] = v[2];
+      store_vd(a, S, i, v);
       mv2 = (double)a.mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
     } else {
       const float4 vf = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
@@ -158,73 +224,71 @@ __global__ void __launch_bounds__(kThreads) k_gauss_b(IntegrateArgs a) {
       mv2 = (double)a.mass[i] * ((double)vf.x * vf.x + (double)vf.y * vf.y + (double)vf.z * vf.z);
     }
   }
-  double m[1] = {mv2}, tot[1];
-  block_sum<1>(m, red);
-  if (last_block_total<1>(m, a.partials, &a.sc->counter[2], tot, red)) {
-    a.sc->mv2 = tot[0];
-    a.sc->xi_old = xi;  // every other block has finished reading xi_old
-    if (!isfinite(tot[0])) atomicOr(a.status, kStatusNonFinite);
+  double s[1] = {mv2}, tot[1];
+  block_sum<1>(s, red);
+  if (sys_total<1>(s, a.partials, blockIdx.x, S.blk0, S.nblk, &sc.counter[2], tot, red)) {
+    sc.mv2 = tot[0];
+    sc.xi_old = xi;  // every other block of this system has finished reading xi_old
+    if (!isfinite(tot[0])) atomicOr(&a.status[m.sys], kStatusNonFinite);
+    count_step(a, m.sys);
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_wrap(IntegrateArgs a) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.N) return;
+__global__ void __launch_bounds__(kIntThreads) k_wrap(IntegrateArgs a) {
+  const BlockMap m = a.map[blockIdx.x];
+  if (threadIdx.x >= m.n) return;
+  const uint32_t i = m.i0 + threadIdx.x;
   float4 p = a.r[i];
-  wrap3(a, p);
+  wrap3(a.sys[m.sys], p);
   a.r[i] = p;
 }
 
-__global__ void __launch_bounds__(kThreads) k_mv2(IntegrateArgs a) {
+__global__ void __launch_bounds__(kIntThreads) k_mv2(IntegrateArgs a) {
   __shared__ double red[32];
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  double m[1] = {0};
-  if (i < a.N) {
-    const float4 v = load_v(a, i);
-    double vx = v.x, vy = v.y, vz = v.z;
-    if (a.vd) {
-      vx = a.vd[i];
-      vy = a.vd[i + a.N];
-      vz = a.vd[i + 2 * a.N];
-    }
-    m[0] = (double)a.mass[i] * (vx * vx + vy * vy + vz * vz);
+  const BlockMap m = a.map[blockIdx.x];
+  const SysInt &S = a.sys[m.sys];
+  double s[1] = {0};
+  if (threadIdx.x < m.n) {
+    const uint32_t i = m.i0 + threadIdx.x;
+    double v[3];
+    load_v(a, S, i, v);
+    s[0] = (double)a.mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
   }
   double tot[1];
-  block_sum<1>(m, red);
-  if (last_block_total<1>(m, a.partials, &a.sc->counter[0], tot, red)) a.sc->mv2 = tot[0];
+  block_sum<1>(s, red);
+  if (sys_total<1>(s, a.partials, blockIdx.x, S.blk0, S.nblk, &a.sc[m.sys].counter[0], tot, red))
+    a.sc[m.sys].mv2 = tot[0];
 }
 
-__global__ void __launch_bounds__(kThreads) k_fv(IntegrateArgs a) {
+__global__ void __launch_bounds__(kIntThreads) k_fv(IntegrateArgs a) {
   __shared__ double red[32];
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  double m[1] = {0};
-  if (i < a.N) {
+  const BlockMap m = a.map[blockIdx.x];
+  const SysInt &S = a.sys[m.sys];
+  double s[1] = {0};
+  if (threadIdx.x < m.n) {
+    const uint32_t i = m.i0 + threadIdx.x;
     const float4 F = a.F[i];
-    double vx, vy, vz;
-    if (a.vd) {
-      vx = a.vd[i];
-      vy = a.vd[i + a.N];
-      vz = a.vd[i + 2 * a.N];
-    } else {
-      const float4 v = a.v[i];
-      vx = v.x;
-      vy = v.y;
-      vz = v.z;
-    }
-    m[0] = (double)F.x * vx + (double)F.y * vy + (double)F.z * vz;
+    double v[3];
+    load_v(a, S, i, v);
+    s[0] = (double)F.x * v[0] + (double)F.y * v[1] + (double)F.z * v[2];
   }
   double tot[1];
-  block_sum<1>(m, red);
-  if (last_block_total<1>(m, a.partials, &a.sc->counter[3], tot, red)) a.sc->fv = tot[0];
+  block_sum<1>(s, red);
+  if (sys_total<1>(s, a.partials, blockIdx.x, S.blk0, S.nblk, &a.sc[m.sys].counter[3], tot, red))
+    a.sc[m.sys].fv = tot[0];
 }
 
-__global__ void __launch_bounds__(kThreads) k_scale(IntegrateArgs a, double s) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.N) return;
+__global__ void __launch_bounds__(kIntThreads) k_scale(IntegrateArgs a, const double *f) {
+  const BlockMap m = a.map[blockIdx.x];
+  if (threadIdx.x >= m.n) return;
+  const SysInt &S = a.sys[m.sys];
+  const uint32_t i = m.i0 + threadIdx.x;
+  const double s = f[m.sys];
   if (a.vd) {
-    a.vd[i] *= s;
-    a.vd[i + a.N] *= s;
-    a.vd[i + 2 * a.N] *= s;
+    double v[3];
+    load_vd(a, S, i, v);
+    for (int k = 0; k < 3; ++k) v[k] *= s;
+    store_vd(a, S, i, v);
   } else {
     const float sf = (float)s;
     float4 v = a.v[i];
@@ -238,22 +302,14 @@ __global__ void __launch_bounds__(kThreads) k_scale(IntegrateArgs a, double s) {
 
 // adjustVelocity_F4 / adjustVelocity_VD (kernelfuncs.cu:546-699): per axis,
 // subtract the mean and scale to standard deviation v1.  Pass 1: sums.
-__global__ void __launch_bounds__(kThreads) k_vstats(IntegrateArgs a) {
+__global__ void __launch_bounds__(kIntThreads) k_vstats(IntegrateArgs a) {
   __shared__ double red[6 * 32];
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const BlockMap m = a.map[blockIdx.x];
+  const SysInt &S = a.sys[m.sys];
   double s[6] = {0, 0, 0, 0, 0, 0};
-  if (i < a.N) {
+  if (threadIdx.x < m.n) {
     double w[3];
-    if (a.vd) {
-      w[0] = a.vd[i];
-      w[1] = a.vd[i + a.N];
-      w[2] = a.vd[i + 2 * a.N];
-    } else {
-      const float4 v = a.v[i];
-      w[0] = v.x;
-      w[1] = v.y;
-      w[2] = v.z;
-    }
+    load_v(a, S, m.i0 + threadIdx.x, w);
     for (int k = 0; k < 3; ++k) {
       s[k] = w[k];
       s[3 + k] = w[k] * w[k];
@@ -261,37 +317,46 @@ __global__ void __launch_bounds__(kThreads) k_vstats(IntegrateArgs a) {
   }
   double tot[6];
   block_sum<6>(s, red);
-  if (last_block_total<6>(s, a.partials, &a.sc->counter[3], tot, red)) {
-    for (int k = 0; k < 6; ++k) a.sc->vstat[k] = tot[k];
+  if (sys_total<6>(s, a.partials, blockIdx.x, S.blk0, S.nblk, &a.sc[m.sys].counter[3], tot, red)) {
+    for (int k = 0; k < 6; ++k) a.sc[m.sys].vstat[k] = tot[k];
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_vapply(IntegrateArgs a, double v1) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.N) return;
-  const double n = (double)a.N;
-  double mean[3], sc[3];
+__global__ void __launch_bounds__(kIntThreads) k_vapply(IntegrateArgs a, const double *v1s) {
+  const BlockMap m = a.map[blockIdx.x];
+  if (threadIdx.x >= m.n) return;
+  const SysInt &S = a.sys[m.sys];
+  const uint32_t i = m.i0 + threadIdx.x;
+  const DevScalars &sc = a.sc[m.sys];
+  const double n = (double)S.natoms, v1 = v1s[m.sys];
+  double mean[3], f[3];
   for (int k = 0; k < 3; ++k) {
-    mean[k] = a.sc->vstat[k] / n;
-    const double var = a.sc->vstat[3 + k] / n - mean[k] * mean[k];
-    sc[k] = var > 0 ? v1 / sqrt(var) : 0.0;
+    mean[k] = sc.vstat[k] / n;
+    const double var = sc.vstat[3 + k] / n - mean[k] * mean[k];
+    f[k] = var > 0 ? v1 / sqrt(var) : 0.0;
   }
   if (a.vd) {
-    for (int k = 0; k < 3; ++k) a.vd[i + k * a.N] = (a.vd[i + k * a.N] - mean[k]) * sc[k];
+    double v[3];
+    load_vd(a, S, i, v);
+    for (int k = 0; k < 3; ++k) v[k] = (v[k] - mean[k]) * f[k];
+    store_vd(a, S, i, v);
   } else {
     float4 v = a.v[i];
-    v.x = (float)((v.x - mean[0]) * sc[0]);
-    v.y = (float)((v.y - mean[1]) * sc[1]);
-    v.z = (float)((v.z - mean[2]) * sc[2]);
+    v.x = (float)((v.x - mean[0]) * f[0]);
+    v.y = (float)((v.y - mean[1]) * f[1]);
+    v.z = (float)((v.z - mean[2]) * f[2]);
     a.v[i] = v;
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_energy_total(const double *partials, uint32_t n,
-                                                          DevScalars *sc) {
+// One block per system: energy partials of the system's force items, in order.
+__global__ void __launch_bounds__(kIntThreads) k_energy_total(const double *partials,
+                                                             const uint32_t *item0,
+                                                             DevScalars *sc) {
   __shared__ double red[4 * 32];
+  const uint32_t s0 = item0[blockIdx.x], s1 = item0[blockIdx.x + 1];
   double s[4] = {0, 0, 0, 0};
-  for (uint32_t b = threadIdx.x; b < n; b += blockDim.x) {
+  for (uint32_t b = s0 + threadIdx.x; b < s1; b += blockDim.x) {
     s[0] += partials[(size_t)b * 4 + 0];
     s[1] += partials[(size_t)b * 4 + 1];
     s[2] += partials[(size_t)b * 4 + 2];
@@ -299,64 +364,66 @@ __global__ void __launch_bounds__(kThreads) k_energy_total(const double *partial
   }
   block_sum<4>(s, red);
   if (threadIdx.x == 0) {
-    sc->pe = s[0];
-    sc->pe_shift = s[1];
-    sc->virial = s[2];
-    sc->npairs = s[3];
+    DevScalars &d = sc[blockIdx.x];
+    d.pe = s[0];
+    d.pe_shift = s[1];
+    d.virial = s[2];
+    d.npairs = s[3];
   }
 }
 
 }  // namespace
 
-uint32_t integrate_blocks(uint32_t N) { return (N + kThreads - 1) / kThreads; }
+uint32_t blocks_for(uint32_t natoms) { return (natoms + kIntThreads - 1) / kIntThreads; }
 
-cudaError_t launch_vv(const IntegrateArgs &a, cudaStream_t s) {
-  if (!a.N) return cudaSuccess;
-  k_vv<<<integrate_blocks(a.N), kThreads, 0, s>>>(a);
-  return cudaGetLastError();
+void make_block_map(const uint32_t *natoms, uint32_t nsys, BlockMap *map, uint32_t *blk0,
+                    uint32_t *nblk) {
+  uint32_t b = 0, atom0 = 0;
+  for (uint32_t s = 0; s < nsys; ++s) {
+    blk0[s] = b;
+    nblk[s] = blocks_for(natoms[s]);
+    for (uint32_t k = 0; k < nblk[s]; ++k) {
+      const uint32_t i0 = atom0 + k * kIntThreads;
+      const uint32_t n = natoms[s] - k * kIntThreads;
+      map[b++] = BlockMap{s, i0, n < (uint32_t)kIntThreads ? n : (uint32_t)kIntThreads, k};
+    }
+    atom0 += natoms[s];
+  }
+}
+
+#define PB_LAUNCH(kern, ...)                                                    \
+  do {                                                                          \
+    if (!a.nblocks) return cudaSuccess;                                         \
+    kern<<<a.nblocks, kIntThreads, 0, s>>>(__VA_ARGS__);                        \
+    return cudaGetLastError();                                                  \
+  } while (0)
+
+cudaError_t launch_vv(const IntegrateArgs &a, cudaStream_t s) { PB_LAUNCH(k_vv, a); }
+cudaError_t launch_wrap(const IntegrateArgs &a, cudaStream_t s) { PB_LAUNCH(k_wrap, a); }
+cudaError_t launch_mv2(const IntegrateArgs &a, cudaStream_t s) { PB_LAUNCH(k_mv2, a); }
+cudaError_t launch_fv(const IntegrateArgs &a, cudaStream_t s) { PB_LAUNCH(k_fv, a); }
+cudaError_t launch_scale(const IntegrateArgs &a, const double *f, cudaStream_t s) {
+  PB_LAUNCH(k_scale, a, f);
 }
 
 cudaError_t launch_gauss(const IntegrateArgs &a, cudaStream_t s) {
-  if (!a.N) return cudaSuccess;
-  k_gauss_a<<<integrate_blocks(a.N), kThreads, 0, s>>>(a);
-  k_gauss_b<<<integrate_blocks(a.N), kThreads, 0, s>>>(a);
+  if (!a.nblocks) return cudaSuccess;
+  k_gauss_a<<<a.nblocks, kIntThreads, 0, s>>>(a);
+  k_gauss_b<<<a.nblocks, kIntThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 
-cudaError_t launch_wrap(const IntegrateArgs &a, cudaStream_t s) {
-  if (!a.N) return cudaSuccess;
-  k_wrap<<<integrate_blocks(a.N), kThreads, 0, s>>>(a);
+cudaError_t launch_adjust(const IntegrateArgs &a, const double *v1, cudaStream_t s) {
+  if (!a.nblocks) return cudaSuccess;
+  k_vstats<<<a.nblocks, kIntThreads, 0, s>>>(a);
+  k_vapply<<<a.nblocks, kIntThreads, 0, s>>>(a, v1);
   return cudaGetLastError();
 }
 
-cudaError_t launch_mv2(const IntegrateArgs &a, cudaStream_t s) {
-  if (!a.N) return cudaSuccess;
-  k_mv2<<<integrate_blocks(a.N), kThreads, 0, s>>>(a);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_fv(const IntegrateArgs &a, cudaStream_t s) {
-  if (!a.N) return cudaSuccess;
-  k_fv<<<integrate_blocks(a.N), kThreads, 0, s>>>(a);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_scale(const IntegrateArgs &a, double factor, cudaStream_t s) {
-  if (!a.N) return cudaSuccess;
-  k_scale<<<integrate_blocks(a.N), kThreads, 0, s>>>(a, factor);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_adjust(const IntegrateArgs &a, double v1, cudaStream_t s) {
-  if (!a.N) return cudaSuccess;
-  k_vstats<<<integrate_blocks(a.N), kThreads, 0, s>>>(a);
-  k_vapply<<<integrate_blocks(a.N), kThreads, 0, s>>>(a, v1);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_energy_total(const double *partials, uint32_t nparts, DevScalars *sc,
-                                cudaStream_t s) {
-  k_energy_total<<<1, kThreads, 0, s>>>(partials, nparts, sc);
+cudaError_t launch_energy_total(const double *partials, const uint32_t *item0, uint32_t nsys,
+                                DevScalars *sc, cudaStream_t s) {
+  if (!nsys) return cudaSuccess;
+  k_energy_total<<<nsys, kIntThreads, 0, s>>>(partials, item0, sc);
   return cudaGetLastError();
 }
 

@@ -1,9 +1,18 @@
-// Time integration and reductions for one system (particle order).
+// Time integration and reductions, for one system or many packed systems.
+//
+// Every CUDA block works on a contiguous atom range of ONE system (the block
+// map below), and every per-system sum is finished by that system's last
+// block, adding the block partials in block order.  The arithmetic an atom
+// sees therefore depends only on its own system, never on which other
+// systems share the launch: a system gives bit-identical results alone and
+// in a batch.
 #pragma once
 
 #include "common.cuh"
 
 namespace pb {
+
+constexpr int kIntThreads = 256;  // atoms per integration block
 
 // Device-resident scalars of one system.  Reductions are finished on the
 // device (last-block pattern), so a step never needs a host round trip.
@@ -20,21 +29,39 @@ struct DevScalars {
   unsigned int counter[4];
 };
 
+// Integration view of one system.
+struct SysInt {
+  uint32_t atom0, natoms;  // atom range in the packed arrays
+  uint32_t vd0;            // start of this system's FP64 velocity planes (x, y, z)
+  uint32_t blk0, nblk;     // its integration blocks
+  float dt;
+  float c0[3], c1[3], L[3];  // box for the wrap
+};
+
+// Block b of an integration launch covers atoms [i0, i0 + n) of system sys;
+// it is block `k` of that system.
+struct BlockMap {
+  uint32_t sys, i0, n, k;
+};
+
 struct IntegrateArgs {
   float4 *r;
   float4 *v;          // FP32 velocities (nullptr when vd is used)
-  double *vd;         // FP64 velocities, SoA planes x[N], y[N], z[N]
+  double *vd;         // FP64 velocities, per-system SoA planes
   const float4 *F;    // F(t)
   const float4 *Fold; // F(t - dt)
   const float *minv;
   const float *mass;
-  uint32_t N;
-  float dt;
-  float c0[3], c1[3], L[3];  // box for the wrap
+  const SysInt *sys;
+  const BlockMap *map;
+  uint32_t nblocks;
   int wrap;
-  DevScalars *sc;
+  DevScalars *sc;     // per system
   double *partials;   // >= 8 doubles per block
-  uint32_t *status;   // status bits (non-finite sums)
+  uint32_t *status;   // status bits, one word per system
+  uint32_t *steps_left;  // per system: steps still to run, 0 = finished and left
+                         // unchanged; decremented by each VV / Gaussian step
+                         // (nullptr: no limit)
 };
 
 cudaError_t launch_vv(const IntegrateArgs &a, cudaStream_t s);
@@ -42,10 +69,18 @@ cudaError_t launch_gauss(const IntegrateArgs &a, cudaStream_t s);
 cudaError_t launch_wrap(const IntegrateArgs &a, cudaStream_t s);
 cudaError_t launch_mv2(const IntegrateArgs &a, cudaStream_t s);
 cudaError_t launch_fv(const IntegrateArgs &a, cudaStream_t s);
-cudaError_t launch_scale(const IntegrateArgs &a, double factor, cudaStream_t s);
-cudaError_t launch_adjust(const IntegrateArgs &a, double v1, cudaStream_t s);
-cudaError_t launch_energy_total(const double *partials, uint32_t nparts, DevScalars *sc,
-                                cudaStream_t s);
-uint32_t integrate_blocks(uint32_t N);
+// Per-system factors / v1 values (device arrays, one double per system).
+cudaError_t launch_scale(const IntegrateArgs &a, const double *factors, cudaStream_t s);
+cudaError_t launch_adjust(const IntegrateArgs &a, const double *v1, cudaStream_t s);
+// Per-system energy totals from force partials: system s owns partials
+// [item0[s], item0[s + 1]) (4 doubles each).
+cudaError_t launch_energy_total(const double *partials, const uint32_t *item0, uint32_t nsys,
+                                DevScalars *sc, cudaStream_t s);
+
+// Host helpers: integration blocks of kIntThreads atoms aligned to each
+// system's first atom.
+uint32_t blocks_for(uint32_t natoms);
+void make_block_map(const uint32_t *natoms, uint32_t nsys, BlockMap *map, uint32_t *blk0,
+                    uint32_t *nblk);
 
 }  // namespace pb

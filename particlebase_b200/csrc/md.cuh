@@ -32,7 +32,7 @@ struct SysDesc {
   uint32_t vd0;             // offset of this system's FP64 velocity planes (3 * atom0)
   uint32_t lj;              // index of this system's LJ table
   float dt;                 // time step
-  float pad;
+  uint32_t cap;             // staged-atom capacity of this system's force CTAs
 };
 
 // Work item of the force kernel: one (x, y) column of one system, z cells
@@ -72,10 +72,11 @@ struct ForceBufs {
   const LJTable *lj;
   const ForceItem *items;
   uint32_t nitems;
-  int cap;                   // staged-atom capacity of a CTA's shared memory
+  int cap;                   // shared-memory capacity of the launch (max over systems)
   float4 *F;                 // force output, particle order
   double *partials;          // per-CTA energy partials (4 doubles per CTA)
   uint32_t *status;
+  const uint32_t *steps_left;  // per system; 0 = finished, skipped (nullptr: all run)
 };
 
 // Launchers (return cudaError_t of the launch).

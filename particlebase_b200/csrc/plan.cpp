@@ -66,10 +66,10 @@ void neighbor_table(const Grid &g, std::vector<uint32_t> &out) {
       }
 }
 
-int choose_segment(double atoms_per_cell, int nz) {
+int choose_segment(double atoms_per_cell, int nz, double scale) {
   // about 160 home atoms (20 clusters of 8) per force CTA; PB_FORCE_SEG overrides
   const double apc = std::max(atoms_per_cell, 1.0);
-  int seg = (int)std::lround(160.0 / apc);
+  int seg = (int)std::lround(160.0 * scale / apc);
   if (const char *e = std::getenv("PB_FORCE_SEG")) seg = std::atoi(e);
   seg = std::max(1, std::min(seg, force_max_segment()));
   return std::min(seg, nz);

@@ -24,9 +24,9 @@ void morton_columns(int nx, int ny, std::vector<uint32_t> &rank, std::vector<uin
 // periodic, in reference cell numbering d2 + d1 nz + d0 nz ny.
 void neighbor_table(const Grid &g, std::vector<uint32_t> &out);
 
-// z cells per force work item for a mean cell occupancy: about 160 home
-// atoms per CTA, at most kMaxSeg (see force.cu).
-int choose_segment(double atoms_per_cell, int nz);
+// z cells per force work item for a mean cell occupancy: about 160 * scale
+// home atoms per CTA, at most kMaxSeg (see force.cu).
+int choose_segment(double atoms_per_cell, int nz, double scale = 1.0);
 
 // Shared-memory capacity (atoms) of a force CTA staging 9 columns x (seg + 2)
 // cells at the given mean occupancy, with headroom for fluctuations.
