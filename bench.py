@@ -336,6 +336,87 @@ def run_ours(args, dist: Dist) -> dict:
     return out
 
 
+def run_batched(args, dist: Dist) -> dict:
+    """256 uneven replicas (N log-uniform in [500, 50,000] as 4k^3 fcc counts,
+    density U[0.70, 0.90], T* U[0.7, 1.5], rc 2.5, Gaussian thermostat, FP32
+    state with FP64 reductions): all replicas in one batch, whole steps
+    replayed from one CUDA graph, force launch shape from the autotuner --
+    against the plain path, the same replicas one pb_md handle at a time."""
+    import torch
+    from particlebase_b200 import workloads as W
+    from particlebase_b200.batch import Batch
+    from particlebase_b200.md import from_system
+    from particlebase_b200.tune import autotune
+
+    steps = args.batch_steps + (args.batch_steps % 2)
+    systems = W.uneven_replicas(args.replicas, seed=3 + dist.rank)
+    natoms = np.array([s.n for s in systems])
+    total = int(natoms.sum())
+    tune = autotune(systems, gaussian=True, dt=DT, steps=6, fp64_velocities=False)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    b = Batch.from_systems(systems, gaussian=True, dt=DT, fp64_velocities=False,
+                           tuning=(tune["threads"], tune["seg_scale"]))
+    b.run(max(2, args.warmup + (args.warmup % 2)))
+    torch.cuda.synchronize()
+    flush.zero_()
+    torch.cuda.synchronize()
+    dist.barrier()
+    batched_ms = b.run_timed(steps)
+    status = int(np.bitwise_or.reduce(b.status()))
+    prof = b.profile(4)
+    b.close()
+    batched_ms = dist.reduce(batched_ms, "max")
+
+    # plain path: every replica in its own handle, graph-replayed, one after another
+    handles = [from_system(s, gaussian=True, fp64_velocities=False) for s in systems]
+    for p in handles:
+        p.run(DT, 2)
+    torch.cuda.synchronize()
+    flush.zero_()
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0 = time.perf_counter()
+    plain_ms = 0.0
+    for p in handles:
+        plain_ms += p.run_timed(DT, steps)
+    plain_wall = time.perf_counter() - t0
+    for p in handles:
+        p.close()
+    plain_ms = dist.reduce(plain_ms, "max")
+
+    # end to end through the public API: host state in, all steps, final positions out
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    q = Batch.from_systems(systems, gaussian=True, dt=DT, fp64_velocities=False,
+                           tuning=(tune["threads"], tune["seg_scale"]))
+    q.run(steps)
+    outs = [q.get(k, "r") for k in range(q.nsys)]
+    e2e_s = time.perf_counter() - t0
+    q.close()
+    e2e_s = dist.reduce(e2e_s, "max")
+
+    v_batched = dist.ws * total * steps / (batched_ms / 1e3)
+    v_plain = dist.ws * total * steps / (plain_ms / 1e3)
+    return {
+        "metric": "batched-replica atom-steps/s (256 uneven LJ replicas)",
+        "value": v_batched, "unit": UNIT, "ms_per_step": batched_ms / steps,
+        "plain_value": v_plain, "plain_ms_per_step": plain_ms / steps,
+        "plain_wall_ms_per_step": plain_wall * 1e3 / steps,
+        "speedup_vs_plain": v_batched / v_plain,
+        "steps": steps, "replicas": len(systems), "atoms": total,
+        "atoms_min": int(natoms.min()), "atoms_max": int(natoms.max()),
+        "tuning": {k: tune[k] for k in ("threads", "seg_scale", "cached")},
+        "phase_ms": prof, "device_status": status,
+        "e2e": {"value": dist.ws * total * steps / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": total * 42 / steps, "d2h_bytes_per_step": total * 16 / steps,
+                "includes": "batch creation from host arrays, all steps, final positions to host"},
+        "config": {"workload": "lj_uneven_replicas_256_gauss", "dt": DT, "seed": 3 + dist.rank,
+                   "plain": "one pb_md handle per replica, 2-step CUDA graphs, sequential",
+                   "l2": "flushed before each timed run; batch state ~0.3 GB > L2"},
+    }
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -344,6 +425,11 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="all", choices=["all", "c2", "c3"],
+                    help="c2: 1M-atom single system; c3: batched replicas; all: c2 line "
+                         "with the c3 result under 'batched'")
+    ap.add_argument("--replicas", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=200)
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)
 
@@ -355,7 +441,14 @@ def main(argv=None) -> int:
 
     dist = Dist(use_cuda=True)
     try:
+        if args.workload == "c3":
+            out = run_batched(args, dist)
+            if dist.rank == 0:
+                print(json.dumps(out), flush=True)
+            return 0
         out = run_ours(args, dist)
+        if args.workload == "all":
+            out["batched"] = run_batched(args, dist)
         if dist.rank == 0:
             if dist.ws == 1 and not args.no_cpu_baseline:
                 out["cpu_baseline"] = run_cpu_oracle(args.cpu_steps)

@@ -301,6 +301,88 @@ int pb_batch_set_tuning(pb_batch *b, int force_threads, float seg_scale);
 int pb_batch_estimate_bytes(const uint32_t *natoms, const float *cells6, const float *rmax,
                             uint32_t nsys, uint32_t flags, size_t *bytes);
 
+/* ---- serving: a request loop over the batch ---------------------------------
+ *
+ * No counterpart in the reference.  A pb_srv owns a scheduler thread and one
+ * resident pb_batch.  Submitted MD jobs wait in a FIFO queue until the
+ * memory estimate of the resident set plus the job fits the HBM budget; the
+ * scheduler then packs them into the batch at the next chunk boundary, where
+ * finished jobs also leave (their final state is copied to host memory).
+ * Between boundaries the batch advances by whole graph-replayed steps, every
+ * job under its own step budget, so each job ends after exactly its step
+ * count, with the result it would have alone (bit for bit, same flags). */
+typedef struct pb_srv pb_srv;
+
+typedef struct pb_srv_config {
+  size_t hbm_budget;      /* bytes the resident batch may hold (estimate); 0 = 90% of free */
+  uint64_t max_atoms;     /* resident atom cap (0 = none): bounds the step time */
+  uint32_t max_jobs;      /* resident job cap (0 = none) */
+  float chunk_ms;         /* target GPU time between chunk boundaries (0 = 50 ms) */
+  uint32_t flags;         /* PB_MD_VEL_FP64 | PB_MD_ACC_FP64 */
+  int mode;               /* PB_MODE_VV or PB_MODE_GAUSS */
+  int force_threads;      /* 0 = default (256) */
+  float seg_scale;        /* 0 = 1.0 */
+} pb_srv_config;
+
+typedef struct pb_srv_job {
+  uint32_t natoms;
+  float cell6[6];
+  float rc;                   /* LJ cutoff (and cell size) */
+  const float *sigma_eps;     /* (sigma, epsilon) per ordered type pair */
+  const float *sigma_eps_rc;  /* optional per-pair cutoffs (sigma, epsilon, rc), or NULL */
+  uint32_t ntypes;
+  float dt, kB;
+  uint32_t steps;
+  const double *r3, *v3, *mass;  /* host arrays, copied by pb_srv_submit; v3/mass may be NULL */
+  const uint32_t *type;          /* or NULL */
+} pb_srv_job;
+
+#define PB_JOB_QUEUED 0
+#define PB_JOB_RUNNING 1
+#define PB_JOB_DONE 2
+#define PB_JOB_FAILED 3
+
+typedef struct pb_srv_job_info {
+  uint64_t id;
+  int state;
+  uint32_t natoms, steps;
+  double t_submit, t_admit, t_done;  /* seconds on the server clock (pb_srv_now) */
+  uint32_t device_status;            /* status bits the kernels raised for this job */
+} pb_srv_job_info;
+
+typedef struct pb_srv_stats {
+  uint64_t submitted, done, failed, rejected;
+  double atom_steps;          /* completed atom-steps of finished jobs */
+  double gpu_seconds;         /* device time of the step chunks (CUDA events) */
+  double repack_seconds;      /* host time spent repacking at chunk boundaries */
+  uint64_t chunks, repacks;
+  uint64_t peak_jobs, peak_atoms;
+  size_t peak_bytes;          /* largest resident-set memory estimate */
+} pb_srv_stats;
+
+int pb_srv_create(const pb_srv_config *cfg, pb_srv **out);
+/* Stops the scheduler (running jobs are abandoned) and frees everything. */
+int pb_srv_destroy(pb_srv *s);
+/* Queue a job; its arrays are copied before the call returns.  A job whose
+ * own memory estimate exceeds the budget is rejected (PB_ERR_OOM). */
+int pb_srv_submit(pb_srv *s, const pb_srv_job *job, uint64_t *id);
+/* Block until job `id` is done or failed (timeout_s < 0: no limit). */
+int pb_srv_wait(pb_srv *s, uint64_t id, double timeout_s);
+/* Block until every submitted job is done or failed. */
+int pb_srv_drain(pb_srv *s, double timeout_s);
+/* Ids of jobs finished since the last poll (up to max). */
+int pb_srv_poll(pb_srv *s, uint64_t *ids, uint32_t max, uint32_t *n);
+int pb_srv_info(pb_srv *s, uint64_t id, pb_srv_job_info *info);
+/* Final state of a finished job: r4 float4[n] positions, v velocities
+ * (float4[n] or double[3n] planes with PB_MD_VEL_FP64, vbytes to match),
+ * F4 float4[n] last forces; any pointer may be NULL. */
+int pb_srv_result(pb_srv *s, uint64_t id, void *r4, void *v, size_t vbytes, void *F4);
+/* Forget a finished job and its stored result. */
+int pb_srv_release(pb_srv *s, uint64_t id);
+int pb_srv_stats_get(pb_srv *s, pb_srv_stats *st);
+double pb_srv_now(const pb_srv *s);
+const char *pb_srv_last_error(const pb_srv *s);
+
 /* Library version string. */
 const char *pb_version(void);
 

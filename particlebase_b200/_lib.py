@@ -43,6 +43,34 @@ class pb_particle(C.Structure):
                 ("is_fixed", C.c_uint8), ("a", C.c_double * 3), ("type", C.c_uint32)]
 
 
+class pb_srv_config(C.Structure):
+    _fields_ = [("hbm_budget", C.c_size_t), ("max_atoms", C.c_uint64), ("max_jobs", C.c_uint32),
+                ("chunk_ms", C.c_float), ("flags", C.c_uint32), ("mode", C.c_int),
+                ("force_threads", C.c_int), ("seg_scale", C.c_float)]
+
+
+class pb_srv_job(C.Structure):
+    _fields_ = [("natoms", C.c_uint32), ("cell6", C.c_float * 6), ("rc", C.c_float),
+                ("sigma_eps", C.c_void_p), ("sigma_eps_rc", C.c_void_p), ("ntypes", C.c_uint32),
+                ("dt", C.c_float), ("kB", C.c_float), ("steps", C.c_uint32),
+                ("r3", C.c_void_p), ("v3", C.c_void_p), ("mass", C.c_void_p),
+                ("type", C.c_void_p)]
+
+
+class pb_srv_job_info(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("state", C.c_int), ("natoms", C.c_uint32),
+                ("steps", C.c_uint32), ("t_submit", C.c_double), ("t_admit", C.c_double),
+                ("t_done", C.c_double), ("device_status", C.c_uint32)]
+
+
+class pb_srv_stats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("done", C.c_uint64), ("failed", C.c_uint64),
+                ("rejected", C.c_uint64), ("atom_steps", C.c_double),
+                ("gpu_seconds", C.c_double), ("repack_seconds", C.c_double),
+                ("chunks", C.c_uint64), ("repacks", C.c_uint64), ("peak_jobs", C.c_uint64),
+                ("peak_atoms", C.c_uint64), ("peak_bytes", C.c_size_t)]
+
+
 class pb_md_sums(C.Structure):
     _fields_ = [("mv2", C.c_double), ("fv", C.c_double), ("pe", C.c_double),
                 ("pe_shift", C.c_double), ("virial", C.c_double), ("xi", C.c_double)]
@@ -116,6 +144,16 @@ def _declare(L: C.CDLL) -> None:
         "pb_batch_set": [vp, u32, i32, vp, C.c_size_t],
         "pb_batch_set_tuning": [vp, i32, f32],
         "pb_batch_estimate_bytes": [vp, vp, vp, u32, u32, C.POINTER(C.c_size_t)],
+        "pb_srv_create": [C.POINTER(pb_srv_config), C.POINTER(vp)],
+        "pb_srv_destroy": [vp],
+        "pb_srv_submit": [vp, C.POINTER(pb_srv_job), C.POINTER(C.c_uint64)],
+        "pb_srv_wait": [vp, C.c_uint64, f64],
+        "pb_srv_drain": [vp, f64],
+        "pb_srv_poll": [vp, vp, u32, C.POINTER(u32)],
+        "pb_srv_info": [vp, C.c_uint64, C.POINTER(pb_srv_job_info)],
+        "pb_srv_result": [vp, C.c_uint64, vp, vp, C.c_size_t, vp],
+        "pb_srv_release": [vp, C.c_uint64],
+        "pb_srv_stats_get": [vp, C.POINTER(pb_srv_stats)],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -125,6 +163,10 @@ def _declare(L: C.CDLL) -> None:
     L.pb_md_last_error.restype = C.c_char_p
     L.pb_batch_last_error.argtypes = [vp]
     L.pb_batch_last_error.restype = C.c_char_p
+    L.pb_srv_last_error.argtypes = [vp]
+    L.pb_srv_last_error.restype = C.c_char_p
+    L.pb_srv_now.argtypes = [vp]
+    L.pb_srv_now.restype = C.c_double
     L.pb_version.restype = C.c_char_p
 
 

@@ -149,3 +149,43 @@ def uneven_replicas(count: int = 256, n_lo: float = 500, n_hi: float = 50_000,
         s = fcc_system(k, d, t, seed=int(rng.integers(1 << 31)), rc=rc, name=f"replica{i}")
         out.append(s)
     return out
+
+
+@dataclass
+class JobSpec:
+    """One served MD job: arrival time (s), fcc cells k (4 k^3 atoms), density,
+    temperature, step count and the seed of its velocities."""
+
+    arrival: float
+    cells: int
+    density: float
+    temperature: float
+    steps: int
+    seed: int
+
+    @property
+    def n(self) -> int:
+        return 4 * self.cells ** 3
+
+    def system(self, rc: float = 2.5) -> LJSystem:
+        return fcc_system(self.cells, self.density, self.temperature, self.seed, rc=rc,
+                          name=f"job_{self.seed}")
+
+
+def served_jobs(count: int = 2000, rate: float = 50.0, n_lo: float = 1_000, n_hi: float = 200_000,
+                rho=(0.75, 0.90), temp=(0.7, 1.2), steps=(100, 5_000),
+                seed: int = 4) -> list[JobSpec]:
+    """Poisson arrival stream of LJ jobs: exponential gaps of mean 1/rate,
+    N log-uniform in [n_lo, n_hi] rounded to a 4k^3 fcc count, density and T*
+    uniform, step count uniform over the integers in `steps`."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for _ in range(count):
+        t += float(rng.exponential(1.0 / rate))
+        n_target = float(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi))))
+        out.append(JobSpec(arrival=t, cells=fcc_cells_for(n_target),
+                           density=float(rng.uniform(*rho)), temperature=float(rng.uniform(*temp)),
+                           steps=int(rng.integers(steps[0], steps[1] + 1)),
+                           seed=int(rng.integers(1 << 31))))
+    return out
