@@ -417,6 +417,64 @@ def run_batched(args, dist: Dist) -> dict:
     }
 
 
+def run_served(args, dist: Dist, jobs: int) -> dict:
+    """Served MD jobs: a Poisson stream (mean 50 jobs/s) of fcc LJ jobs with N
+    log-uniform in [1,000, 200,000] (as 4k^3 counts), density U[0.75, 0.90],
+    T* U[0.7, 1.2], steps U[100, 5,000], Gaussian thermostat, submitted in
+    real time to the job server under a 120 GB HBM budget.  Latency = done -
+    submitted on the server clock (queueing included); throughput = completed
+    atom-steps / (last completion - first submission)."""
+    import torch
+    from particlebase_b200 import workloads as W
+    from particlebase_b200.serve import Server
+
+    specs = W.served_jobs(count=jobs, seed=4 + dist.rank)
+    free, _ = torch.cuda.mem_get_info()
+    budget = min(120e9, 0.8 * free)
+    srv = Server(hbm_budget=budget, gaussian=True, fp64_velocities=False, chunk_ms=args.chunk_ms)
+    dist.barrier()
+    t0 = time.perf_counter()
+    ids = []
+    lag = 0.0
+    for sp in specs:
+        delay = sp.arrival - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        else:
+            lag = max(lag, -delay)
+        ids.append(srv.submit(sp.system(), sp.steps, DT))
+    srv.drain()
+    infos = [srv.info(i) for i in ids]
+    st = srv.stats()
+    srv.close()
+    lat = np.array([i["t_done"] - i["t_submit"] for i in infos])
+    wait = np.array([i["t_admit"] - i["t_submit"] for i in infos])
+    span = max(i["t_done"] for i in infos) - min(i["t_submit"] for i in infos)
+    atom_steps = float(sum(sp.n * sp.steps for sp in specs))
+    status = 0
+    for i in infos:
+        status |= i["device_status"]
+    value = dist.reduce(atom_steps, "sum") / dist.reduce(span, "max")
+    return {
+        "metric": "served MD jobs: aggregate atom-steps/s and p50/p99 job latency",
+        "value": value, "unit": UNIT,
+        "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+        "p50_admission_wait_s": float(np.percentile(wait, 50)),
+        "p99_admission_wait_s": float(np.percentile(wait, 99)),
+        "jobs": len(specs), "done": st["done"], "failed": st["failed"],
+        "atom_steps": atom_steps, "span_s": span,
+        "gpu_busy_fraction": st["gpu_seconds"] / span if span > 0 else None,
+        "gpu_atom_steps_per_s": atom_steps / st["gpu_seconds"] if st["gpu_seconds"] else None,
+        "repacks": st["repacks"], "repack_s": st["repack_seconds"], "chunks": st["chunks"],
+        "peak_jobs": st["peak_jobs"], "peak_atoms": st["peak_atoms"],
+        "peak_bytes": st["peak_bytes"], "hbm_budget_bytes": budget,
+        "submit_lag_s": lag, "device_status": status,
+        "config": {"workload": f"lj_served_poisson50_{len(specs)}jobs_gauss", "dt": DT,
+                   "seed": 4 + dist.rank, "chunk_ms": args.chunk_ms,
+                   "note": "all 2,000 jobs with --workload c4 --jobs 2000"},
+    }
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -425,9 +483,13 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="all", choices=["all", "c2", "c3"],
-                    help="c2: 1M-atom single system; c3: batched replicas; all: c2 line "
-                         "with the c3 result under 'batched'")
+    ap.add_argument("--workload", default="all", choices=["all", "c2", "c3", "c4"],
+                    help="c2: 1M-atom single system; c3: batched replicas; c4: served jobs; "
+                         "all: the c2 line with c3 under 'batched' and a c4 sample under "
+                         "'served'")
+    ap.add_argument("--jobs", type=int, default=None,
+                    help="served jobs (default: 2000 with --workload c4, 200 in 'all')")
+    ap.add_argument("--chunk-ms", type=float, default=50.0)
     ap.add_argument("--replicas", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=200)
     args = ap.parse_args(argv)
@@ -441,14 +503,16 @@ def main(argv=None) -> int:
 
     dist = Dist(use_cuda=True)
     try:
-        if args.workload == "c3":
-            out = run_batched(args, dist)
+        if args.workload in ("c3", "c4"):
+            out = (run_batched(args, dist) if args.workload == "c3"
+                   else run_served(args, dist, args.jobs or 2000))
             if dist.rank == 0:
                 print(json.dumps(out), flush=True)
             return 0
         out = run_ours(args, dist)
         if args.workload == "all":
             out["batched"] = run_batched(args, dist)
+            out["served"] = run_served(args, dist, args.jobs or 200)
         if dist.rank == 0:
             if dist.ws == 1 and not args.no_cpu_baseline:
                 out["cpu_baseline"] = run_cpu_oracle(args.cpu_steps)

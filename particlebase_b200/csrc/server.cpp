@@ -12,8 +12,8 @@
 //      their device state bit for bit, new jobs are imported, cells are set up
 //      and every job's remaining step count becomes its step budget;
 //   4. the batch advances by K whole steps (graph replays), K chosen so a
-//      chunk takes about chunk_ms of GPU time but no longer than the longest
-//      remaining job needs.
+//      chunk takes about max(chunk_ms, 4 x the last repack time) of GPU time
+//      but no longer than the longest remaining job needs.
 // Jobs whose budget ends inside a chunk simply stop there (the kernels skip
 // them), so every job runs exactly its own step count.
 #include <algorithm>
@@ -76,6 +76,7 @@ struct pb_srv {
   pb_batch *batch = nullptr;
   std::vector<Job *> slots;  // job of each batch system
   double ms_per_atom_step = 5e-7;
+  double last_repack_ms = 0.0;
   std::thread worker;
 
   double now() const {
@@ -261,8 +262,10 @@ void scheduler(pb_srv *s) {
           j->t_admit = t;
         }
         ++s->st.repacks;
-        s->st.repack_seconds +=
+        const double sec =
             std::chrono::duration<double>(std::chrono::steady_clock::now() - t_r).count();
+        s->st.repack_seconds += sec;
+        s->last_repack_ms = 1e3 * sec;
       }
       if (rc) {
         fail_resident(s, why);
@@ -278,7 +281,10 @@ void scheduler(pb_srv *s) {
       atoms += j->n;
       longest = std::max(longest, j->remaining);
     }
-    const double chunk_ms = s->cfg.chunk_ms > 0 ? s->cfg.chunk_ms : 50.0;
+    // a chunk lasts at least four repacks, so repacking costs at most a fifth
+    // of the GPU time even when jobs arrive and leave at every boundary
+    const double chunk_ms =
+        std::max(s->cfg.chunk_ms > 0 ? (double)s->cfg.chunk_ms : 50.0, 4.0 * s->last_repack_ms);
     double want = chunk_ms / std::max(1e-6, s->ms_per_atom_step * (double)atoms);
     uint32_t K = (uint32_t)std::max(2.0, std::min(want, 1e6));
     K += K & 1u;
