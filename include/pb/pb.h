@@ -179,6 +179,12 @@ int pb_md_scale_velocities(pb_md *h, double s);
 /* adjustVelocities (cudaParticleMD.cu:177-198, GaussianThermo.cu:98-119):
  * zero mean per axis, standard deviation v1 per axis. */
 int pb_md_adjust_velocities(pb_md *h, double v1);
+/* constTemp's force correction (cudaParticleMD.cu:140-155, correctConstTemp_F4
+ * kernelfuncs.cu:533-544): F -= lambda m v on the latest force. */
+int pb_md_correct_force(pb_md *h, double lambda);
+/* Gaussian friction xi carried into the next step (GaussianThermo::xi),
+ * e.g. when restoring a checkpoint. */
+int pb_md_set_xi(pb_md *h, double xi);
 /* Mean particle mass m0 of the last import (cudaParticleMD.cu:327-336). */
 int pb_md_mean_mass(const pb_md *h, double *m0);
 

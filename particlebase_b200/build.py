@@ -110,12 +110,72 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+SHIM = os.path.join(PKG, "shim")
+DRIVERS = os.path.join(SHIM, "_drivers")
+MD_DRIVERS = ("testMD1", "testMD2", "testMD3", "testMD4")
+
+
+def reference_dir() -> str:
+    return os.environ.get("PB_REFERENCE_DIR", "/root/reference")
+
+
+def build_drivers(names=MD_DRIVERS, ref_dir: str | None = None, force: bool = False) -> list[str]:
+    """Compile the reference's MD drivers, unmodified, against the drop-in
+    classes in shim/ and this library.  Each driver source is reached through a
+    symlink in shim/_drivers, so its quoted includes ("CUDAenv.hh", ...) find
+    the shim headers rather than the headers next to the original file.
+    Returns the built executables (none when the reference checkout is absent)."""
+    ref = ref_dir or reference_dir()
+    if not os.path.isdir(ref):
+        return []
+    build()
+    os.makedirs(DRIVERS, exist_ok=True)
+    cc = nvcc()
+    shim_dig = _digest(sorted(os.path.join(dp, f) for dp, _, fs in os.walk(SHIM)
+                              if "_drivers" not in dp for f in fs if f.endswith((".hh", ".h", ".hpp"))), LIB)
+
+    def one(name: str) -> str | None:
+        src = os.path.join(ref, name + ".cu")
+        if not os.path.exists(src):
+            return None
+        link = os.path.join(DRIVERS, name + ".cu")
+        if os.path.islink(link) or os.path.exists(link):
+            os.remove(link)
+        os.symlink(src, link)
+        exe = os.path.join(DRIVERS, name)
+        stamp = exe + ".stamp"
+        dig = _digest([src], shim_dig)
+        if not force and os.path.exists(exe) and os.path.exists(stamp) and open(stamp).read() == dig:
+            os.remove(link)
+            return exe
+        cmd = [cc, "-ccbin", host_cxx(), *ARCH, "-O2", "-std=c++17", "-DREAL=float",
+               "-I", SHIM, "-I", os.path.join(ROOT, "include"), link, "-o", exe,
+               "-L", LIBDIR, "-lparticlebase_b200", "-Xlinker", "-rpath", "-Xlinker",
+               "$ORIGIN/../../lib"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        os.remove(link)  # the executable is what ships; the link points outside the tree
+        if r.returncode != 0:
+            raise RuntimeError(f"driver {name} failed to build:\n{r.stdout}\n{r.stderr}")
+        with open(stamp, "w") as fh:
+            fh.write(dig)
+        return exe
+
+    with cf.ThreadPoolExecutor(max_workers=4) as ex:
+        out = [x for x in ex.map(one, names) if x]
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--drivers", action="store_true",
+                    help="also compile the reference MD drivers against the drop-in classes")
     a = ap.parse_args(argv)
     print(build(force=a.force, verbose=a.verbose))
+    if a.drivers:
+        for exe in build_drivers(force=a.force):
+            print(exe)
     return 0
 
 

@@ -642,6 +642,23 @@ int engine_adjust(Engine &e, const double *v1) {
   return PB_OK;
 }
 
+int engine_correct_force(Engine &e, const double *lambda) {
+  E_CUDA(cudaMemcpyAsync(e.d_fac, lambda, sizeof(double) * e.nsys, cudaMemcpyHostToDevice,
+                         e.stream));
+  cudaError_t c = launch_correct_force(engine_iargs(e, 0), e.F[e.last], e.d_fac, e.stream);
+  if (c != cudaSuccess) return cuda_fail(e, c, "correct force");
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  return PB_OK;
+}
+
+int engine_set_xi(Engine &e, const double *xi) {
+  for (uint32_t s = 0; s < e.nsys; ++s)
+    E_CUDA(cudaMemcpyAsync(&e.sc[s].xi_old, &xi[s], sizeof(double), cudaMemcpyHostToDevice,
+                           e.stream));
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  return PB_OK;
+}
+
 int engine_scalars(Engine &e, std::vector<DevScalars> &out) {
   out.resize(e.nsys);
   E_CUDA(cudaMemcpyAsync(out.data(), e.sc, sizeof(DevScalars) * e.nsys, cudaMemcpyDeviceToHost,

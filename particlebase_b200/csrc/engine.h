@@ -109,6 +109,8 @@ int engine_mv2(Engine &e);
 int engine_fv(Engine &e);
 int engine_scale(Engine &e, const double *factors);
 int engine_adjust(Engine &e, const double *v1);
+int engine_correct_force(Engine &e, const double *lambda);
+int engine_set_xi(Engine &e, const double *xi);
 int engine_scalars(Engine &e, std::vector<DevScalars> &out);
 int engine_status(Engine &e, std::vector<uint32_t> &bits);
 void engine_drop_graph(Engine &e);

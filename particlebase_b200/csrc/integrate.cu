@@ -349,6 +349,24 @@ __global__ void __launch_bounds__(kIntThreads) k_vapply(IntegrateArgs a, const d
   }
 }
 
+// correctConstTemp_F4 (kernelfuncs.cu:533-544): F -= lambda m v, per system.
+__global__ void __launch_bounds__(kIntThreads) k_correct(IntegrateArgs a, float4 *F,
+                                                        const double *lambda) {
+  const BlockMap m = a.map[blockIdx.x];
+  if (threadIdx.x >= m.n) return;
+  const SysInt &S = a.sys[m.sys];
+  const uint32_t i = m.i0 + threadIdx.x;
+  double v[3];
+  load_v(a, S, i, v);
+  const float l = (float)lambda[m.sys];
+  const float mi = a.mass[i];
+  float4 f = F[i];
+  f.x -= l * mi * (float)v[0];
+  f.y -= l * mi * (float)v[1];
+  f.z -= l * mi * (float)v[2];
+  F[i] = f;
+}
+
 // One block per system: energy partials of the system's force items, in order.
 __global__ void __launch_bounds__(kIntThreads) k_energy_total(const double *partials,
                                                              const uint32_t *item0,
@@ -418,6 +436,11 @@ cudaError_t launch_adjust(const IntegrateArgs &a, const double *v1, cudaStream_t
   k_vstats<<<a.nblocks, kIntThreads, 0, s>>>(a);
   k_vapply<<<a.nblocks, kIntThreads, 0, s>>>(a, v1);
   return cudaGetLastError();
+}
+
+cudaError_t launch_correct_force(const IntegrateArgs &a, float4 *F, const double *lambda,
+                                 cudaStream_t s) {
+  PB_LAUNCH(k_correct, a, F, lambda);
 }
 
 cudaError_t launch_energy_total(const double *partials, const uint32_t *item0, uint32_t nsys,

@@ -72,6 +72,9 @@ cudaError_t launch_fv(const IntegrateArgs &a, cudaStream_t s);
 // Per-system factors / v1 values (device arrays, one double per system).
 cudaError_t launch_scale(const IntegrateArgs &a, const double *factors, cudaStream_t s);
 cudaError_t launch_adjust(const IntegrateArgs &a, const double *v1, cudaStream_t s);
+// F -= lambda[sys] m v on the force buffer `F` (constTemp).
+cudaError_t launch_correct_force(const IntegrateArgs &a, float4 *F, const double *lambda,
+                                 cudaStream_t s);
 // Per-system energy totals from force partials: system s owns partials
 // [item0[s], item0[s + 1]) (4 doubles each).
 cudaError_t launch_energy_total(const double *partials, const uint32_t *item0, uint32_t nsys,

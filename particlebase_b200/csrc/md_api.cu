@@ -292,6 +292,12 @@ int pb_md_adjust_velocities(pb_md *h, double v1) {
   return h ? engine_adjust(h->e, &v1) : PB_ERR_ARG;
 }
 
+int pb_md_correct_force(pb_md *h, double lambda) {
+  return h ? engine_correct_force(h->e, &lambda) : PB_ERR_ARG;
+}
+
+int pb_md_set_xi(pb_md *h, double xi) { return h ? engine_set_xi(h->e, &xi) : PB_ERR_ARG; }
+
 int pb_md_mean_mass(const pb_md *h, double *m0) {
   if (!h || !m0) return PB_ERR_ARG;
   *m0 = h->p().m0;
