@@ -475,6 +475,48 @@ def run_served(args, dist: Dist, jobs: int) -> dict:
     }
 
 
+def run_kob_andersen(args, dist: Dist) -> dict:
+    """Kob-Andersen 80:20 binary mixture, 8,388,608 atoms at density 1.2 from
+    uniform random positions, relaxed by 200 capped steepest-descent iterations
+    on the GPU (untimed preparation), then a Gaussian thermostat at T* 0.8 with
+    FP32 state and FP64 reductions; K timed steps, per-pair cutoffs 2.5 sigma_ab."""
+    import torch
+    from particlebase_b200 import workloads as W
+    from particlebase_b200.md import from_system
+
+    s = W.config_c5(seed=5 + dist.rank, n=args.ka_atoms)
+    p = from_system(s, gaussian=True, fp64_velocities=False)
+    t0 = time.perf_counter()
+    p.minimize(200, 1e-3, 0.02)
+    relax_s = time.perf_counter() - t0
+    p.clearForce()
+    p.adjustVelocities(0.8)
+    p.run(DT, max(2, args.warmup + (args.warmup % 2)))
+    torch.cuda.synchronize()
+    steps = args.ka_steps + (args.ka_steps % 2)
+    dist.barrier()
+    ms = p.run_timed(DT, steps)
+    ms = dist.reduce(ms, "max")
+    T = p.calcTemp()
+    status = p.status()
+    prof = p.profile(DT, 4)
+    p.calcBlockID()
+    p.calcForce(energy=True)
+    ps = p.pair_stats()
+    sums = p.sums()
+    p.close()
+    return {
+        "metric": "LJ atom-steps/s, Kob-Andersen 8.4M atoms", "unit": UNIT,
+        "value": dist.ws * s.n * steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps,
+        "atoms": s.n, "relax_s": relax_s, "temperature": T, "pe_per_atom": sums["pe"] / s.n,
+        "phase_ms": prof, "ncand_per_atom": ps["ncand"] / s.n, "nin_per_atom": ps["nin"] / s.n,
+        "flops_per_atom_step": (8 * ps["ncand"] + 14 * ps["nin"]) / s.n,
+        "device_status": status,
+        "config": {"workload": f"kob_andersen_{s.n}_rho1.2_T0.8_gauss", "dt": DT,
+                   "relax": "200 capped steepest-descent iterations (alpha 1e-3, max 0.02 sigma)"},
+    }
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -483,13 +525,15 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="all", choices=["all", "c2", "c3", "c4"],
+    ap.add_argument("--workload", default="all", choices=["all", "c2", "c3", "c4", "c5"],
                     help="c2: 1M-atom single system; c3: batched replicas; c4: served jobs; "
                          "all: the c2 line with c3 under 'batched' and a c4 sample under "
                          "'served'")
     ap.add_argument("--jobs", type=int, default=None,
                     help="served jobs (default: 2000 with --workload c4, 200 in 'all')")
     ap.add_argument("--chunk-ms", type=float, default=50.0)
+    ap.add_argument("--ka-atoms", type=int, default=8_388_608)
+    ap.add_argument("--ka-steps", type=int, default=300)
     ap.add_argument("--replicas", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=200)
     args = ap.parse_args(argv)
@@ -503,9 +547,10 @@ def main(argv=None) -> int:
 
     dist = Dist(use_cuda=True)
     try:
-        if args.workload in ("c3", "c4"):
-            out = (run_batched(args, dist) if args.workload == "c3"
-                   else run_served(args, dist, args.jobs or 2000))
+        if args.workload in ("c3", "c4", "c5"):
+            out = {"c3": lambda: run_batched(args, dist),
+                   "c4": lambda: run_served(args, dist, args.jobs or 2000),
+                   "c5": lambda: run_kob_andersen(args, dist)}[args.workload]()
             if dist.rank == 0:
                 print(json.dumps(out), flush=True)
             return 0
@@ -513,6 +558,7 @@ def main(argv=None) -> int:
         if args.workload == "all":
             out["batched"] = run_batched(args, dist)
             out["served"] = run_served(args, dist, args.jobs or 200)
+            out["kob_andersen"] = run_kob_andersen(args, dist)
         if dist.rank == 0:
             if dist.ws == 1 and not args.no_cpu_baseline:
                 out["cpu_baseline"] = run_cpu_oracle(args.cpu_steps)

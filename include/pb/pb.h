@@ -182,6 +182,12 @@ int pb_md_adjust_velocities(pb_md *h, double v1);
 /* constTemp's force correction (cudaParticleMD.cu:140-155, correctConstTemp_F4
  * kernelfuncs.cu:533-544): F -= lambda m v on the latest force. */
 int pb_md_correct_force(pb_md *h, double lambda);
+/* Extension (no counterpart in the reference): steepest-descent relaxation of
+ * overlapping starts, `iters` times: cell build, relaxation force (pair
+ * distance floored at sigma/2 so forces stay finite), then every atom moves by
+ * F min(alpha, max_disp / |F|) and wraps.  F afterwards holds the relaxation
+ * force; call pb_md_clear_force before dynamics. */
+int pb_md_minimize(pb_md *h, uint32_t iters, float alpha, float max_disp);
 /* Gaussian friction xi carried into the next step (GaussianThermo::xi),
  * e.g. when restoring a checkpoint. */
 int pb_md_set_xi(pb_md *h, double xi);

@@ -164,7 +164,7 @@ struct ForceOut {
 void compute_forces(const double *r3, const uint32_t *type, uint32_t N, const double *L,
                     const Grid &g, const uint32_t *nbr, const uint32_t *start,
                     const uint32_t *members, const uint32_t *cid, const LJTable &t,
-                    double *F3, double *pe_atom, ForceOut &out) {
+                    double *F3, double *pe_atom, ForceOut &out, bool capped = false) {
   double pe = 0, pes = 0, vir = 0, nc = 0, ni = 0;
   const int nt = t.ntypes;
 #pragma omp parallel for schedule(dynamic, 64) reduction(+ : pe, pes, vir, nc, ni)
@@ -189,9 +189,12 @@ void compute_forces(const double *r3, const uint32_t *type, uint32_t N, const do
         const int k = ti * nt + (int)type[j];
         if (r2 < t.rc2[k]) {
           ni += 1;
-          const double sr2 = t.s2[k] / r2;
+          // relaxation force (extension): r^2 floored at (sigma/2)^2 so that
+          // overlapping random starts give finite forces
+          const double r2f = capped ? std::max(r2, 0.25 * t.s2[k]) : r2;
+          const double sr2 = t.s2[k] / r2f;
           const double sr6 = sr2 * sr2 * sr2;
-          const double f = t.e24[k] * sr6 * (2.0 * sr6 - 1.0) / r2;
+          const double f = t.e24[k] * sr6 * (2.0 * sr6 - 1.0) / r2f;
           fx += f * dx;
           fy += f * dy;
           fz += f * dz;
@@ -251,10 +254,10 @@ void build_cells(System &s) {
   cell_list(cid.data(), nullptr, s.N, s.g.ncells, s.start.data(), s.members.data());
 }
 
-void forces(System &s) {
+void forces(System &s, bool capped = false) {
   build_cells(s);
   compute_forces(s.r.data(), s.type.data(), s.N, s.L, s.g, s.nbr.data(), s.start.data(),
-                 s.members.data(), s.cid.data(), s.t, s.F.data(), s.pe_atom.data(), s.fo);
+                 s.members.data(), s.cid.data(), s.t, s.F.data(), s.pe_atom.data(), s.fo, capped);
 }
 
 void wrap_all(System &s) {
@@ -511,24 +514,23 @@ int orc_run(void *h, uint32_t steps, double dt, int mode, double *energy_out) {
 }
 
 // Extension (not in the reference): steepest-descent relaxation used to
-// prepare random Kob-Andersen configurations.  Each iteration moves every
-// atom along its force by gamma * F, with gamma chosen so that the largest
-// displacement is max_disp.
-void orc_steepest_descent(void *h, uint32_t iters, double max_disp) {
+// prepare random Kob-Andersen configurations.  Each iteration evaluates the
+// relaxation force (pair distance floored at sigma/2) and moves every atom by
+// F * min(alpha, max_disp / |F|): a plain gradient step, capped at max_disp
+// per atom so that overlapping pairs separate without flinging atoms away.
+void orc_steepest_descent(void *h, uint32_t iters, double alpha, double max_disp) {
   System &s = *(System *)h;
   for (uint32_t it = 0; it < iters; ++it) {
-    forces(s);
-    double fmax2 = 0;
-#pragma omp parallel for schedule(static) reduction(max : fmax2)
-    for (long i = 0; i < (long)s.N; ++i) {
-      const double f2 = s.F[3 * i] * s.F[3 * i] + s.F[3 * i + 1] * s.F[3 * i + 1] +
-                        s.F[3 * i + 2] * s.F[3 * i + 2];
-      fmax2 = std::max(fmax2, f2);
-    }
-    if (fmax2 <= 0) break;
-    const double gamma = max_disp / std::sqrt(fmax2);
+    forces(s, true);
 #pragma omp parallel for schedule(static)
-    for (long q = 0; q < (long)(3 * s.N); ++q) s.r[q] += gamma * s.F[q];
+    for (long i = 0; i < (long)s.N; ++i) {
+      const double fx = s.F[3 * i], fy = s.F[3 * i + 1], fz = s.F[3 * i + 2];
+      const double f = std::sqrt(fx * fx + fy * fy + fz * fz);
+      const double g = f * alpha > max_disp ? max_disp / f : alpha;
+      s.r[3 * i] += g * fx;
+      s.r[3 * i + 1] += g * fy;
+      s.r[3 * i + 2] += g * fz;
+    }
     wrap_all(s);
   }
 }

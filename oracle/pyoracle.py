@@ -69,7 +69,7 @@ def lib() -> C.CDLL:
         L.orc_forces.argtypes = [C.c_void_p, _f64p]
         L.orc_run.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_int, C.c_void_p]
         L.orc_run.restype = C.c_int
-        L.orc_steepest_descent.argtypes = [C.c_void_p, C.c_uint32, C.c_double]
+        L.orc_steepest_descent.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double]
         L.orc_kinetic.argtypes = [C.c_void_p]
         L.orc_kinetic.restype = C.c_double
         L.orc_get_xi.argtypes = [C.c_void_p]
@@ -212,8 +212,10 @@ class Oracle:
     def set_fold(self, fold):
         lib().orc_set_fold(self.h, np.ascontiguousarray(fold, np.float64).reshape(-1))
 
-    def steepest_descent(self, iters, max_disp):
-        lib().orc_steepest_descent(self.h, iters, max_disp)
+    def steepest_descent(self, iters, alpha, max_disp):
+        """Capped steepest descent (extension): r += F min(alpha, max_disp/|F|)
+        with the relaxation force (pair distance floored at sigma/2)."""
+        lib().orc_steepest_descent(self.h, iters, alpha, max_disp)
 
     def get(self, name):
         idx = {"r": 0, "v": 1, "F": 2, "Fold": 3, "pe_atom": 4}[name]

@@ -642,6 +642,25 @@ int engine_adjust(Engine &e, const double *v1) {
   return PB_OK;
 }
 
+int engine_minimize(Engine &e, uint32_t iters, float alpha, float max_disp) {
+  if (!engine_ready(e)) return fail(e, PB_ERR_STATE, "need cell, LJ parameters and setup_cells");
+  if (!(alpha > 0) || !(max_disp > 0)) return fail(e, PB_ERR_ARG, "alpha and max_disp must be > 0");
+  int nt = 1;
+  for (const auto &P : e.sp) nt = std::max(nt, P.lj.nt);
+  for (uint32_t it = 0; it < iters; ++it) {
+    int rc = engine_build(e);
+    if (rc) return rc;
+    cudaError_t c = launch_force_capped(engine_fbufs(e), nt, e.stream);
+    if (c != cudaSuccess) return cuda_fail(e, c, "relaxation force");
+    e.last = e.cur;
+    c = launch_sd_move(engine_iargs(e, 1), e.F[e.cur], alpha, max_disp, e.stream);
+    if (c != cudaSuccess) return cuda_fail(e, c, "steepest descent");
+  }
+  e.energy_valid = false;
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  return PB_OK;
+}
+
 int engine_correct_force(Engine &e, const double *lambda) {
   E_CUDA(cudaMemcpyAsync(e.d_fac, lambda, sizeof(double) * e.nsys, cudaMemcpyHostToDevice,
                          e.stream));

@@ -110,6 +110,8 @@ int engine_fv(Engine &e);
 int engine_scale(Engine &e, const double *factors);
 int engine_adjust(Engine &e, const double *v1);
 int engine_correct_force(Engine &e, const double *lambda);
+// Steepest-descent relaxation: iters x (cell build, relaxation force, move).
+int engine_minimize(Engine &e, uint32_t iters, float alpha, float max_disp);
 int engine_set_xi(Engine &e, const double *xi);
 int engine_scalars(Engine &e, std::vector<DevScalars> &out);
 int engine_status(Engine &e, std::vector<uint32_t> &bits);

@@ -64,13 +64,16 @@ struct Stage {
   int shifted;         // any nonzero frame shift in this CTA
 };
 
-template <int NT, bool ENERGY, typename Acc>
+// CAP: relaxation force of the steepest-descent path, with the pair distance
+// floored at sigma/2 so that overlapping random starts give finite forces.
+template <int NT, bool ENERGY, typename Acc, bool CAP = false>
 struct PairAcc {
   Acc fx = 0, fy = 0, fz = 0, pe = 0, pes = 0, vir = 0;
   uint32_t n = 0;
   template <int M>
   __device__ __forceinline__ void add(const LJLocal<M> &lj, int k, float dx, float dy, float dz,
                                       float r2) {
+    if (CAP) r2 = fmaxf(r2, 0.25f * lj.s2[k]);
     const float inv = rcp_approx(r2);
     const float sr2 = lj.s2[k] * inv;
     const float sr6 = sr2 * sr2 * sr2;
@@ -90,11 +93,12 @@ struct PairAcc {
 
 // Global-memory path (stage overflow): lanes are 32 consecutive home atoms,
 // candidates of one z cell of one column, frame shifts applied per pair.
-template <int NT, bool ENERGY, bool SELF, typename Acc>
+template <int NT, bool ENERGY, bool SELF, typename Acc, bool CAP>
 __device__ __forceinline__ void global_range(const float4 *__restrict__ P, uint32_t jb,
                                              uint32_t je, float xi, float yi, float zi, int ti,
                                              float sx, float sy, float sz, uint32_t self,
-                                             const LJLocal<NT> &lj, PairAcc<NT, ENERGY, Acc> &a) {
+                                             const LJLocal<NT> &lj,
+                                             PairAcc<NT, ENERGY, Acc, CAP> &a) {
   for (uint32_t j = jb; j < je; ++j) {
     const float4 q = P[j];
     const float dx = xi - (q.x - sx), dy = yi - (q.y - sy), dz = zi - (q.z - sz);
@@ -122,10 +126,10 @@ __device__ __forceinline__ uint32_t upper_bound_z(const float4 *sp, uint32_t lo,
   return lo;
 }
 
-template <int NT, bool ENERGY, typename Acc>
+template <int NT, bool ENERGY, typename Acc, bool CAP>
 __device__ __forceinline__ void flush_list(const float4 *sp, const uint16_t *list, uint32_t cnt,
                                            int lane, float4 pi, int ti, const LJLocal<NT> &lj,
-                                           PairAcc<NT, ENERGY, Acc> &a) {
+                                           PairAcc<NT, ENERGY, Acc, CAP> &a) {
   if constexpr (NT == 1) {
     LJLocal<1> r;  // one type: parameters in registers
     r.s2[0] = lj.s2[0];
@@ -150,7 +154,7 @@ __device__ __forceinline__ void flush_list(const float4 *sp, const uint16_t *lis
   }
 }
 
-template <int NT, bool ENERGY, typename Acc, int kWarps>
+template <int NT, bool ENERGY, typename Acc, int kWarps, bool CAP>
 __global__ void __launch_bounds__(kWarps * 32) k_force(ForceBufs b) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint16_t *lists = reinterpret_cast<uint16_t *>(smem_raw);                  // kWarps*kListLen*32
@@ -320,7 +324,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_force(ForceBufs b) {
                             : upper_bound_z(sp, lo, hi, zmax + rcw);
         }
       }
-      PairAcc<NT, ENERGY, Acc> acc;
+      PairAcc<NT, ENERGY, Acc, CAP> acc;
       uint32_t cnt = 0;
       for (int c = 0; c < 9; ++c) {
         const uint32_t jlo = __shfl_sync(0xffffffffu, bound, c);
@@ -331,7 +335,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_force(ForceBufs b) {
           const uint32_t je = min(jhi, jb + 4 * kListLen);
           const uint32_t need = (je - jb + 3) >> 2;
           if (__reduce_max_sync(0xffffffffu, cnt) + need > (uint32_t)kListLen) {
-            flush_list<NT, ENERGY, Acc>(sp, mylist, cnt, lane, pi, ti, ljs, acc);
+            flush_list<NT, ENERGY, Acc, CAP>(sp, mylist, cnt, lane, pi, ti, ljs, acc);
             cnt = 0;
             __syncwarp();
           }
@@ -368,7 +372,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_force(ForceBufs b) {
           cnt = (uint32_t)(out - (mylist + lane)) >> 5;
         }
       }
-      flush_list<NT, ENERGY, Acc>(sp, mylist, cnt, lane, pi, ti, ljs, acc);
+      flush_list<NT, ENERGY, Acc, CAP>(sp, mylist, cnt, lane, pi, ti, ljs, acc);
       __syncwarp();
       // combine the 4 partial sums of each home atom (lanes il, il+8, il+16, il+24)
 #pragma unroll
@@ -406,17 +410,17 @@ __global__ void __launch_bounds__(kWarps * 32) k_force(ForceBufs b) {
       const float4 p = b.rs[gh];
       const float xi = p.x - st.sx[4], yi = p.y - st.sy[4], zi = p.z - st.sz_mid;
       const int ti = NT == 1 ? 0 : __float_as_int(p.w);
-      PairAcc<NT, ENERGY, Acc> acc;
+      PairAcc<NT, ENERGY, Acc, CAP> acc;
       for (int c = 0; c < 9; ++c) {
         for (int k = kmin - 1; k <= kmax + 1; ++k) {
           const int zc = (z0 - 1 + k + nz) % nz;
           const uint32_t key = st.kbase[c] + (uint32_t)zc;
           const float sz = k == 0 ? st.sz_lo : (k == nseg + 1 ? st.sz_hi : st.sz_mid);
           if (c == 4)
-            global_range<NT, ENERGY, true, Acc>(b.rs, b.start[key], b.start[key + 1], xi, yi, zi,
+            global_range<NT, ENERGY, true, Acc, CAP>(b.rs, b.start[key], b.start[key + 1], xi, yi, zi,
                                                 ti, st.sx[c], st.sy[c], sz, gh, ljs, acc);
           else
-            global_range<NT, ENERGY, false, Acc>(b.rs, b.start[key], b.start[key + 1], xi, yi,
+            global_range<NT, ENERGY, false, Acc, CAP>(b.rs, b.start[key], b.start[key + 1], xi, yi,
                                                  zi, ti, st.sx[c], st.sy[c], sz, 0, ljs, acc);
         }
       }
@@ -443,10 +447,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_force(ForceBufs b) {
   }
 }
 
-template <int NT, bool E, typename Acc, int W>
+template <int NT, bool E, typename Acc, int W, bool CAP = false>
 cudaError_t launch_w(const ForceBufs &b, cudaStream_t s) {
   const size_t smem = (size_t)W * kListLen * 32 * 2 + (size_t)b.cap * sizeof(float4);
-  auto kern = k_force<NT, E, Acc, W>;
+  auto kern = k_force<NT, E, Acc, W, CAP>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   kern<<<b.nitems, W * 32, smem, s>>>(b);
@@ -470,6 +474,16 @@ cudaError_t launch_nt(const ForceBufs &b, bool energy, bool acc64, int warps, cu
 
 int force_max_segment() { return kMaxSeg; }
 int force_threads() { return kDefaultWarps * 32; }
+
+cudaError_t launch_force_capped(const ForceBufs &b, int nt_max, cudaStream_t s) {
+  if (b.nitems == 0) return cudaSuccess;
+  switch (nt_max) {
+    case 1: return launch_w<1, false, float, kDefaultWarps, true>(b, s);
+    case 2: return launch_w<2, false, float, kDefaultWarps, true>(b, s);
+    case 3: case 4: return launch_w<4, false, float, kDefaultWarps, true>(b, s);
+    default: return launch_w<8, false, float, kDefaultWarps, true>(b, s);
+  }
+}
 
 cudaError_t launch_force(const ForceBufs &b, int nt_max, bool energy, bool acc64,
                          int block_threads, cudaStream_t s) {

@@ -349,6 +349,25 @@ __global__ void __launch_bounds__(kIntThreads) k_vapply(IntegrateArgs a, const d
   }
 }
 
+// Steepest-descent move (extension, no counterpart in the reference): each
+// atom goes along its force by F min(alpha, max_disp / |F|), then wraps.
+__global__ void __launch_bounds__(kIntThreads) k_sd_move(IntegrateArgs a, const float4 *F,
+                                                        float alpha, float max_disp) {
+  const BlockMap m = a.map[blockIdx.x];
+  if (threadIdx.x >= m.n) return;
+  const SysInt &S = a.sys[m.sys];
+  const uint32_t i = m.i0 + threadIdx.x;
+  const float4 f = F[i];
+  const float fn = sqrtf(fmaf(f.x, f.x, fmaf(f.y, f.y, f.z * f.z)));
+  const float g = fn * alpha > max_disp ? max_disp / fn : alpha;
+  float4 p = a.r[i];
+  p.x = fmaf(g, f.x, p.x);
+  p.y = fmaf(g, f.y, p.y);
+  p.z = fmaf(g, f.z, p.z);
+  wrap3(S, p);
+  a.r[i] = p;
+}
+
 // correctConstTemp_F4 (kernelfuncs.cu:533-544): F -= lambda m v, per system.
 __global__ void __launch_bounds__(kIntThreads) k_correct(IntegrateArgs a, float4 *F,
                                                         const double *lambda) {
@@ -436,6 +455,11 @@ cudaError_t launch_adjust(const IntegrateArgs &a, const double *v1, cudaStream_t
   k_vstats<<<a.nblocks, kIntThreads, 0, s>>>(a);
   k_vapply<<<a.nblocks, kIntThreads, 0, s>>>(a, v1);
   return cudaGetLastError();
+}
+
+cudaError_t launch_sd_move(const IntegrateArgs &a, const float4 *F, float alpha, float max_disp,
+                           cudaStream_t s) {
+  PB_LAUNCH(k_sd_move, a, F, alpha, max_disp);
 }
 
 cudaError_t launch_correct_force(const IntegrateArgs &a, float4 *F, const double *lambda,

@@ -83,5 +83,7 @@ struct ForceBufs {
 cudaError_t launch_cell_build(const CellBufs &b, cudaStream_t s);
 cudaError_t launch_force(const ForceBufs &b, int nt_max, bool energy, bool acc64,
                          int block_threads, cudaStream_t s);
+// Relaxation force for steepest descent: pair distance floored at sigma/2.
+cudaError_t launch_force_capped(const ForceBufs &b, int nt_max, cudaStream_t s);
 
 }  // namespace pb

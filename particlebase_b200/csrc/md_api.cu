@@ -296,6 +296,10 @@ int pb_md_correct_force(pb_md *h, double lambda) {
   return h ? engine_correct_force(h->e, &lambda) : PB_ERR_ARG;
 }
 
+int pb_md_minimize(pb_md *h, uint32_t iters, float alpha, float max_disp) {
+  return h ? engine_minimize(h->e, iters, alpha, max_disp) : PB_ERR_ARG;
+}
+
 int pb_md_set_xi(pb_md *h, double xi) { return h ? engine_set_xi(h->e, &xi) : PB_ERR_ARG; }
 
 int pb_md_mean_mass(const pb_md *h, double *m0) {

@@ -182,6 +182,12 @@ class MDSystem:
         self._ck(self.lib.pb_md_profile(self.h, C.c_float(dt), mode, int(steps), ms), "profile")
         return {"cells": ms[0], "force": ms[1], "evolve": ms[2]}
 
+    def minimize(self, iters: int, alpha: float = 1e-3, max_disp: float = 0.02) -> None:
+        """Extension: capped steepest descent (r += F min(alpha, max_disp/|F|)) with
+        the relaxation force; used to relax random starts before dynamics."""
+        self._ck(self.lib.pb_md_minimize(self.h, int(iters), C.c_float(alpha),
+                                         C.c_float(max_disp)), "minimize")
+
     def pair_stats(self) -> dict:
         out = (C.c_double * 2)()
         self._ck(self.lib.pb_md_pair_stats(self.h, out), "pair_stats")

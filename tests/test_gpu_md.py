@@ -131,7 +131,7 @@ def test_force_1m_vs_oracle(cuda_lib, po):
 def test_force_kob_andersen_per_pair_cutoff(cuda_lib, po):
     s = W.kob_andersen_random(6000, 1.2, 0.8, seed=4)
     O = po.Oracle(s.box, s.lj, s.rc, s.r, s.v, types=s.types)
-    O.steepest_descent(60, 0.02)
+    O.steepest_descent(60, 1e-3, 0.02)
     s.r = O.get("r").astype(np.float32).astype(np.float64)
     p = md(cuda_lib, s)
     p.calcBlockID()
@@ -342,3 +342,22 @@ def test_errors_are_returned_not_fatal(cuda_lib):
     assert e.value.code == 1
     with pytest.raises(L.PBError):
         p.setupCutoffBlock(1.0, periodic=False)
+
+
+def test_minimize_matches_oracle(cuda_lib, po):
+    """Capped steepest descent (extension) on the GPU follows the oracle's
+    relaxation from a random Kob-Andersen start, and removes the overlaps."""
+    s = W.kob_andersen_random(4000, 1.2, 0.8, seed=6)
+    s.r = s.r.astype(np.float32).astype(np.float64)
+    p = md(cuda_lib, s)
+    O = po.Oracle(s.box, s.lj, s.rc, s.r, s.v, types=s.types)
+    p.minimize(10, 1e-3, 0.02)
+    O.steepest_descent(10, 1e-3, 0.02)
+    d = p.get("r")[:, :3].astype(np.float64) - O.get("r")
+    d -= np.round(d / s.L) * s.L
+    assert np.abs(d).max() < 1e-3
+    p.minimize(190, 1e-3, 0.02)
+    p.calcBlockID()
+    p.calcForce(energy=True)
+    assert p.status() == 0
+    assert p.sums()["pe"] / s.n < -4.0  # the random start is far above zero

@@ -227,7 +227,7 @@ def test_kob_andersen_forces_vs_reference_kernel(po):
     """Two-type system with one global cutoff (the reference has no per-pair rc)."""
     s = W.kob_andersen_random(3000, 1.2, 0.8, seed=3)
     O = po.Oracle(s.box, s.lj, s.rc, s.r, s.v, types=s.types)
-    O.steepest_descent(30, 0.02)
+    O.steepest_descent(30, 1e-3, 0.02)
     r = O.get("r")
     lj_global = s.lj.copy()
     lj_global[..., 2] = 2.5
