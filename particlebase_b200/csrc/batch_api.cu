@@ -119,6 +119,7 @@ int pb_batch_repack(const pb_batch *old, const int32_t *src, const uint32_t *nat
                                  cudaMemcpyDeviceToHost) != cudaSuccess)
     return bail(PB_ERR_CUDA);
   e.last = o.last ^ o.cur;  // new F[k] is old F[k ^ o.cur]
+  std::vector<GatherSrc> gs(nsys, GatherSrc{-1, 0, 0, 0});
   std::memset(nsc.data(), 0, sizeof(DevScalars) * nsys);
   for (uint32_t k = 0; k < nsys; ++k) {
     if (src[k] < 0) continue;
@@ -143,27 +144,43 @@ int pb_batch_repack(const pb_batch *old, const int32_t *src, const uint32_t *nat
     // coincide after a completed step)
     const bool fin = engine_finished(o, s);
     const int fb = engine_force_buffer(o, s);
-    struct Copy {
-      void *dst;
-      const void *src;
-      size_t bytes;
-    } copies[] = {
-        {e.r + na, o.r + oa, 16 * cnt},
-        {e.F[0] + na, o.F[fin ? fb : o.cur] + oa, 16 * cnt},
-        {e.F[1] + na, o.F[fin ? fb : 1 - o.cur] + oa, 16 * cnt},
-        {e.minv + na, o.minv + oa, 4 * cnt},
-        {e.mass + na, o.mass + oa, 4 * cnt},
-        {e.type + na, o.type + oa, 2 * cnt},
-        {e.v ? (void *)(e.v + na) : nullptr, o.v ? (const void *)(o.v + oa) : nullptr, 16 * cnt},
-        {e.vd ? (void *)(e.vd + 3 * na) : nullptr, o.vd ? (const void *)(o.vd + 3 * oa) : nullptr,
-         24 * cnt},
-    };
-    for (const Copy &c : copies) {
-      if (!c.dst || !c.src) continue;
-      if (cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToDevice, e.stream) != cudaSuccess)
-        return bail(PB_ERR_CUDA);
-    }
+    gs[k].src = (int32_t)s;
+    gs[k].o_atom0 = (uint32_t)oa;
+    gs[k].fb0 = (uint8_t)(fin ? fb : o.cur);
+    gs[k].fb1 = (uint8_t)(fin ? fb : 1 - o.cur);
+    (void)na;
+    (void)cnt;
   }
+  // all continuing systems' per-atom state in one launch
+  GatherSrc *d_gs = nullptr;
+  if (cudaMallocAsync((void **)&d_gs, sizeof(GatherSrc) * nsys, e.stream) != cudaSuccess ||
+      cudaMemcpyAsync(d_gs, gs.data(), sizeof(GatherSrc) * nsys, cudaMemcpyHostToDevice,
+                      e.stream) != cudaSuccess)
+    return bail(PB_ERR_CUDA);
+  GatherArgs ga{};
+  ga.map = e.d_map;
+  ga.sys = e.d_sysint;
+  ga.nblocks = e.nblocks;
+  ga.gs = d_gs;
+  ga.o_r = o.r;
+  ga.o_v = o.v;
+  ga.o_F0 = o.F[0];
+  ga.o_F1 = o.F[1];
+  ga.o_vd = o.vd;
+  ga.o_minv = o.minv;
+  ga.o_mass = o.mass;
+  ga.o_type = o.type;
+  ga.r = e.r;
+  ga.v = e.v;
+  ga.F0 = e.F[0];
+  ga.F1 = e.F[1];
+  ga.vd = e.vd;
+  ga.minv = e.minv;
+  ga.mass = e.mass;
+  ga.type = e.type;
+  const cudaError_t gc = launch_gather_state(ga, e.stream);
+  cudaFreeAsync(d_gs, e.stream);
+  if (gc != cudaSuccess) return bail(PB_ERR_CUDA);
   if (cudaMemcpyAsync(e.sc, nsc.data(), sizeof(DevScalars) * nsys, cudaMemcpyHostToDevice,
                       e.stream) != cudaSuccess ||
       cudaStreamSynchronize(e.stream) != cudaSuccess)

@@ -4,6 +4,10 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
 
 #include "../../include/pb/pb.h"
 #include "plan.h"
@@ -26,34 +30,92 @@ int cuda_fail(Engine &e, cudaError_t c, const char *what) {
     if (c_ != cudaSuccess) return cuda_fail(e, c_, #call); \
   } while (0)
 
-template <typename T>
-cudaError_t dalloc(T **p, size_t count) {
-  if (count == 0) count = 1;
-  return cudaMalloc((void **)p, sizeof(T) * count);
+// Engine memory comes from a stream-ordered pool per device that keeps up to
+// kPoolKeep bytes of freed memory, so the batches a server builds and drops at
+// every repack reuse memory instead of going back to the driver.
+constexpr uint64_t kPoolKeep = 8ull << 30;
+
+cudaMemPool_t device_pool() {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = pools.find(dev);
+  if (it != pools.end()) return it->second;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+  uint64_t keep = kPoolKeep;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  pools[dev] = pool;
+  return pool;
 }
 
 template <typename T>
-void dfree(T *&p) {
-  if (p) cudaFree((void *)p);
+cudaError_t dalloc(Engine &e, T **p, size_t count) {
+  if (count == 0) count = 1;
+  cudaMemPool_t pool = device_pool();
+  if (!pool) return cudaErrorMemoryAllocation;
+  return cudaMallocFromPoolAsync((void **)p, sizeof(T) * count, pool, e.stream);
+}
+
+template <typename T>
+void dfree(Engine &e, T *&p) {
+  if (p) cudaFreeAsync((void *)p, e.stream);
   p = nullptr;
 }
 
+// Column ranking and force work items depend only on the grid and the z-run
+// length; batches of many similar systems share them.
+struct PlanKey {
+  int nx, ny, nz, seg;
+  bool operator<(const PlanKey &o) const {
+    return std::tie(nx, ny, nz, seg) < std::tie(o.nx, o.ny, o.nz, o.seg);
+  }
+};
+struct Plan {
+  std::vector<uint32_t> rank, xy;
+  std::vector<ForceItem> items;  // system 0, cell0 0
+};
+
+std::shared_ptr<const Plan> cached_plan(const Grid &g, int seg) {
+  static std::mutex mu;
+  static std::map<PlanKey, std::shared_ptr<const Plan>> cache;
+  const PlanKey k{g.n[0], g.n[1], g.n[2], seg};
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(k);
+    if (it != cache.end()) return it->second;
+  }
+  auto p = std::make_shared<Plan>();
+  morton_columns(g.n[0], g.n[1], p->rank, p->xy);
+  append_items(0, g, seg, 0, p->rank, p->xy, p->items);
+  std::lock_guard<std::mutex> lk(mu);
+  if (cache.size() > 4096) cache.clear();
+  cache[k] = p;
+  return p;
+}
+
 void free_cells(Engine &e) {
-  dfree(e.key);
-  dfree(e.within);
-  dfree(e.count);
-  dfree(e.start);
-  dfree(e.tilesum);
-  dfree(e.pid_tmp);
-  dfree(e.pid);
-  dfree(e.slot);
-  dfree(e.rs);
-  dfree(e.colrank);
-  dfree(e.colxy);
-  dfree(e.d_sys);
-  dfree(e.d_items);
-  dfree(e.d_item0);
-  dfree(e.fpartials);
+  dfree(e, e.key);
+  dfree(e, e.within);
+  dfree(e, e.count);
+  dfree(e, e.start);
+  dfree(e, e.tilesum);
+  dfree(e, e.pid_tmp);
+  dfree(e, e.pid);
+  dfree(e, e.slot);
+  dfree(e, e.rs);
+  dfree(e, e.colrank);
+  dfree(e, e.colxy);
+  dfree(e, e.d_sys);
+  dfree(e, e.d_items);
+  dfree(e, e.d_item0);
+  dfree(e, e.fpartials);
   e.cells_ready = false;
 }
 
@@ -107,18 +169,18 @@ int engine_init(Engine &e, const uint32_t *natoms, uint32_t nsys, uint32_t flags
     }
   }
   const uint32_t N = e.N;
-  bool ok = dalloc(&e.r, N) == cudaSuccess && dalloc(&e.F[0], N) == cudaSuccess &&
-            dalloc(&e.F[1], N) == cudaSuccess && dalloc(&e.minv, N) == cudaSuccess &&
-            dalloc(&e.mass, N) == cudaSuccess && dalloc(&e.type, N) == cudaSuccess &&
-            dalloc(&e.d_sysint, nsys) == cudaSuccess && dalloc(&e.d_map, e.nblocks) == cudaSuccess &&
-            dalloc(&e.ipartials, (size_t)8 * e.nblocks) == cudaSuccess &&
-            dalloc(&e.sc, nsys) == cudaSuccess && dalloc(&e.status, nsys) == cudaSuccess &&
-            dalloc(&e.d_fac, nsys) == cudaSuccess && dalloc(&e.d_lj, nsys) == cudaSuccess;
+  bool ok = dalloc(e, &e.r, N) == cudaSuccess && dalloc(e, &e.F[0], N) == cudaSuccess &&
+            dalloc(e, &e.F[1], N) == cudaSuccess && dalloc(e, &e.minv, N) == cudaSuccess &&
+            dalloc(e, &e.mass, N) == cudaSuccess && dalloc(e, &e.type, N) == cudaSuccess &&
+            dalloc(e, &e.d_sysint, nsys) == cudaSuccess && dalloc(e, &e.d_map, e.nblocks) == cudaSuccess &&
+            dalloc(e, &e.ipartials, (size_t)8 * e.nblocks) == cudaSuccess &&
+            dalloc(e, &e.sc, nsys) == cudaSuccess && dalloc(e, &e.status, nsys) == cudaSuccess &&
+            dalloc(e, &e.d_fac, nsys) == cudaSuccess && dalloc(e, &e.d_lj, nsys) == cudaSuccess;
   if (flags & PB_MD_VEL_FP64)
-    ok = ok && dalloc(&e.vd, (size_t)3 * N) == cudaSuccess;
+    ok = ok && dalloc(e, &e.vd, (size_t)3 * N) == cudaSuccess;
   else
-    ok = ok && dalloc(&e.v, N) == cudaSuccess;
-  if (nsys > 1) ok = ok && dalloc(&e.sysid, N) == cudaSuccess;
+    ok = ok && dalloc(e, &e.v, N) == cudaSuccess;
+  if (nsys > 1) ok = ok && dalloc(e, &e.sysid, N) == cudaSuccess;
   if (!ok) return fail(e, PB_ERR_OOM, "device allocation failed");
   E_CUDA(cudaMemsetAsync(e.r, 0, sizeof(float4) * N, e.stream));
   E_CUDA(cudaMemsetAsync(e.F[0], 0, sizeof(float4) * N, e.stream));
@@ -130,13 +192,7 @@ int engine_init(Engine &e, const uint32_t *natoms, uint32_t nsys, uint32_t flags
   E_CUDA(cudaMemsetAsync(e.status, 0, sizeof(uint32_t) * nsys, e.stream));
   E_CUDA(cudaMemcpyAsync(e.d_map, map.data(), sizeof(BlockMap) * e.nblocks, cudaMemcpyHostToDevice,
                          e.stream));
-  if (e.sysid) {
-    std::vector<uint32_t> sid(N);
-    for (uint32_t s = 0; s < nsys; ++s)
-      for (uint32_t i = e.atom0[s]; i < e.atom0[s + 1]; ++i) sid[i] = s;
-    E_CUDA(cudaMemcpyAsync(e.sysid, sid.data(), 4 * (size_t)N, cudaMemcpyHostToDevice, e.stream));
-    E_CUDA(cudaStreamSynchronize(e.stream));
-  }
+  if (e.sysid) E_CUDA(launch_fill_sysid(e.d_map, e.nblocks, e.sysid, e.stream));
   if (const char *t = std::getenv("PB_FORCE_THREADS")) e.force_threads = std::atoi(t);
   int rc = engine_upload_sysint(e);
   if (rc) return rc;
@@ -148,23 +204,23 @@ void engine_free(Engine &e) {
   if (e.stream) cudaStreamSynchronize(e.stream);
   engine_drop_graph(e);
   free_cells(e);
-  dfree(e.r);
-  dfree(e.v);
-  dfree(e.vd);
-  dfree(e.F[0]);
-  dfree(e.F[1]);
-  dfree(e.minv);
-  dfree(e.mass);
-  dfree(e.type);
-  dfree(e.sysid);
-  dfree(e.d_sysint);
-  dfree(e.d_map);
-  dfree(e.ipartials);
-  dfree(e.sc);
-  dfree(e.status);
-  dfree(e.d_fac);
-  dfree(e.d_lj);
-  dfree(e.steps_left);
+  dfree(e, e.r);
+  dfree(e, e.v);
+  dfree(e, e.vd);
+  dfree(e, e.F[0]);
+  dfree(e, e.F[1]);
+  dfree(e, e.minv);
+  dfree(e, e.mass);
+  dfree(e, e.type);
+  dfree(e, e.sysid);
+  dfree(e, e.d_sysint);
+  dfree(e, e.d_map);
+  dfree(e, e.ipartials);
+  dfree(e, e.sc);
+  dfree(e, e.status);
+  dfree(e, e.d_fac);
+  dfree(e, e.d_lj);
+  dfree(e, e.steps_left);
   if (e.own_stream && e.stream) cudaStreamDestroy(e.stream);
   e.stream = nullptr;
 }
@@ -305,21 +361,30 @@ int engine_setup_cells(Engine &e) {
     P.seg = choose_segment(apc, g.n[2], e.seg_scale);
     P.cap = (uint32_t)choose_capacity(apc, P.seg);
     e.cap_max = std::max(e.cap_max, P.cap);
-    std::vector<uint32_t> rank, xy;
-    morton_columns(g.n[0], g.n[1], rank, xy);
+    const std::shared_ptr<const Plan> plan_ref = cached_plan(g, P.seg);
+    const Plan &plan = *plan_ref;
+    const std::vector<uint32_t> &rank = plan.rank, &xy = plan.xy;
     e.cell0[s] = (uint32_t)ncells;
     e.item0[s] = (uint32_t)items.size();
-    append_items(s, g, P.seg, (uint32_t)ncells, rank, xy, items);
-    P.key_of_ref.assign(g.ncells, 0);
-    P.ref_of_key.assign(g.ncells, 0);
-    for (int d0 = 0; d0 < g.n[0]; ++d0)
-      for (int d1 = 0; d1 < g.n[1]; ++d1)
-        for (int d2 = 0; d2 < g.n[2]; ++d2) {
-          const uint32_t ref = d2 + d1 * g.n[2] + d0 * g.n[2] * g.n[1];
-          const uint32_t key = rank[d0 * g.n[1] + d1] * g.n[2] + d2;
-          P.key_of_ref[ref] = key;
-          P.ref_of_key[key] = ref;
-        }
+    for (ForceItem it : plan.items) {  // the system's items: its index and first cell key
+      it.sys = s;
+      for (auto &k : it.kbase) k += (uint32_t)ncells;
+      items.push_back(it);
+    }
+    P.key_of_ref.clear();
+    P.ref_of_key.clear();
+    if (e.nsys == 1) {  // reference cell id <-> key, for the single-system getters
+      P.key_of_ref.assign(g.ncells, 0);
+      P.ref_of_key.assign(g.ncells, 0);
+      for (int d0 = 0; d0 < g.n[0]; ++d0)
+        for (int d1 = 0; d1 < g.n[1]; ++d1)
+          for (int d2 = 0; d2 < g.n[2]; ++d2) {
+            const uint32_t ref = d2 + d1 * g.n[2] + d0 * g.n[2] * g.n[1];
+            const uint32_t key = rank[d0 * g.n[1] + d1] * g.n[2] + d2;
+            P.key_of_ref[ref] = key;
+            P.ref_of_key[key] = ref;
+          }
+    }
     SysDesc &D = sd[s];
     D.g = g;
     D.atom0 = e.atom0[s];
@@ -341,15 +406,15 @@ int engine_setup_cells(Engine &e) {
   e.nitems = (uint32_t)items.size();
   const uint32_t N = e.N, C = e.ncells;
   const uint32_t ntiles = (C + 4095) / 4096;
-  bool ok = dalloc(&e.key, N) == cudaSuccess && dalloc(&e.within, N) == cudaSuccess &&
-            dalloc(&e.count, C) == cudaSuccess && dalloc(&e.start, (size_t)C + 1) == cudaSuccess &&
-            dalloc(&e.tilesum, ntiles) == cudaSuccess && dalloc(&e.pid_tmp, N) == cudaSuccess &&
-            dalloc(&e.pid, N) == cudaSuccess && dalloc(&e.slot, N) == cudaSuccess &&
-            dalloc(&e.rs, N) == cudaSuccess && dalloc(&e.colrank, rank_all.size()) == cudaSuccess &&
-            dalloc(&e.colxy, xy_all.size()) == cudaSuccess &&
-            dalloc(&e.d_sys, e.nsys) == cudaSuccess && dalloc(&e.d_items, items.size()) == cudaSuccess &&
-            dalloc(&e.d_item0, e.nsys + 1) == cudaSuccess &&
-            dalloc(&e.fpartials, (size_t)4 * items.size()) == cudaSuccess;
+  bool ok = dalloc(e, &e.key, N) == cudaSuccess && dalloc(e, &e.within, N) == cudaSuccess &&
+            dalloc(e, &e.count, C) == cudaSuccess && dalloc(e, &e.start, (size_t)C + 1) == cudaSuccess &&
+            dalloc(e, &e.tilesum, ntiles) == cudaSuccess && dalloc(e, &e.pid_tmp, N) == cudaSuccess &&
+            dalloc(e, &e.pid, N) == cudaSuccess && dalloc(e, &e.slot, N) == cudaSuccess &&
+            dalloc(e, &e.rs, N) == cudaSuccess && dalloc(e, &e.colrank, rank_all.size()) == cudaSuccess &&
+            dalloc(e, &e.colxy, xy_all.size()) == cudaSuccess &&
+            dalloc(e, &e.d_sys, e.nsys) == cudaSuccess && dalloc(e, &e.d_items, items.size()) == cudaSuccess &&
+            dalloc(e, &e.d_item0, e.nsys + 1) == cudaSuccess &&
+            dalloc(e, &e.fpartials, (size_t)4 * items.size()) == cudaSuccess;
   if (!ok) {
     free_cells(e);
     return fail(e, PB_ERR_OOM, "cell list allocation failed");
@@ -569,13 +634,13 @@ int engine_set_steps_left(Engine &e, const uint32_t *steps) {
   if (!steps) {
     if (e.steps_left) {
       E_CUDA(cudaStreamSynchronize(e.stream));
-      dfree(e.steps_left);
+      dfree(e, e.steps_left);
       engine_drop_graph(e);  // captured launches hold the old pointer
     }
     return PB_OK;
   }
   if (!e.steps_left) {
-    if (dalloc(&e.steps_left, e.nsys) != cudaSuccess) return fail(e, PB_ERR_OOM, "steps_left");
+    if (dalloc(e, &e.steps_left, e.nsys) != cudaSuccess) return fail(e, PB_ERR_OOM, "steps_left");
     engine_drop_graph(e);  // captured launches hold the old (null) pointer
   }
   e.budget_set.assign(e.nsys, e.steps_done);

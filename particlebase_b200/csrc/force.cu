@@ -43,7 +43,7 @@ namespace {
 
 constexpr int kMaxSeg = 40;     // longest z run of one work item (cells)
 constexpr int kDefaultWarps = 8;
-constexpr int kListLen = 24;    // per-lane pair list entries before a flush
+constexpr int kListLen = 32;    // per-lane pair list entries before a flush
 
 template <int NT>
 struct LJLocal {
@@ -155,7 +155,7 @@ __device__ __forceinline__ void flush_list(const float4 *sp, const uint16_t *lis
 }
 
 template <int NT, bool ENERGY, typename Acc, int kWarps, bool CAP>
-__global__ void __launch_bounds__(kWarps * 32) k_force(ForceBufs b) {
+__global__ void __launch_bounds__(kWarps * 32, 32 / kWarps) k_force(ForceBufs b) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint16_t *lists = reinterpret_cast<uint16_t *>(smem_raw);                  // kWarps*kListLen*32
   float4 *sp = reinterpret_cast<float4 *>(smem_raw + kWarps * kListLen * 32 * 2);
@@ -308,6 +308,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_force(ForceBufs b) {
       const bool valid = h < H;
       const uint32_t hs = hbeg + (valid ? h : H - 1);
       const float4 pi = sp[hs];
+      const float2 pxy = make_float2(pi.x, pi.y);
+      const float2 m1 = make_float2(-1.0f, -1.0f);
       const int ti = NT == 1 ? 0 : __float_as_int(pi.w);
       // cutoff^2 of this lane's pairs; a padded lane gets -1 and never appends
       float rc2_1 = NT == 1 ? ljs.rc2[0] : 0.f;
@@ -348,25 +350,29 @@ __global__ void __launch_bounds__(kWarps * 32) k_force(ForceBufs b) {
 #pragma unroll 4
             for (int t = 0; t < n; ++t, j += 4) {
               const float4 qj = pj[4 * t];
-              const float dx = pi.x - qj.x, dy = pi.y - qj.y, dz = pi.z - qj.z;
-              const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+              // x and y differences as one packed FP32x2 pair (p - q exactly, FMA by -1)
+              const float2 dxy = __ffma2_rn(make_float2(qj.x, qj.y), m1, pxy);
+              const float2 sq = __fmul2_rn(dxy, dxy);
+              const float dz = pi.z - qj.z;
+              const float r2 = fmaf(dz, dz, sq.x + sq.y);
               const float rc2 = NT == 1 ? rc2_1 : (valid ? ljs.rc2[ti * NT + __float_as_int(qj.w)] : -1.f);
-              if (r2 < rc2 && j != hs) {
-                *out = (uint16_t)j;
-                out += 32;
-              }
+              // the store is in bounds whether or not it is kept: the chunk
+              // check above leaves room for every candidate of this chunk
+              *out = (uint16_t)j;
+              out += (r2 < rc2 && j != hs) ? 32 : 0;
             }
           } else {
 #pragma unroll 4
             for (int t = 0; t < n; ++t, j += 4) {
               const float4 qj = pj[4 * t];
-              const float dx = pi.x - qj.x, dy = pi.y - qj.y, dz = pi.z - qj.z;
-              const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+              // x and y differences as one packed FP32x2 pair (p - q exactly, FMA by -1)
+              const float2 dxy = __ffma2_rn(make_float2(qj.x, qj.y), m1, pxy);
+              const float2 sq = __fmul2_rn(dxy, dxy);
+              const float dz = pi.z - qj.z;
+              const float r2 = fmaf(dz, dz, sq.x + sq.y);
               const float rc2 = NT == 1 ? rc2_1 : (valid ? ljs.rc2[ti * NT + __float_as_int(qj.w)] : -1.f);
-              if (r2 < rc2) {
-                *out = (uint16_t)j;
-                out += 32;
-              }
+              *out = (uint16_t)j;
+              out += (r2 < rc2) ? 32 : 0;
             }
           }
           cnt = (uint32_t)(out - (mylist + lane)) >> 5;

@@ -409,7 +409,48 @@ __global__ void __launch_bounds__(kIntThreads) k_energy_total(const double *part
   }
 }
 
+__global__ void __launch_bounds__(kIntThreads) k_fill_sysid(const BlockMap *map, uint32_t *sysid) {
+  const BlockMap m = map[blockIdx.x];
+  if (threadIdx.x < m.n) sysid[m.i0 + threadIdx.x] = m.sys;
+}
+
+__global__ void __launch_bounds__(kIntThreads) k_gather_state(GatherArgs g) {
+  const BlockMap m = g.map[blockIdx.x];
+  const GatherSrc q = g.gs[m.sys];
+  if (q.src < 0 || threadIdx.x >= m.n) return;
+  const uint32_t off = m.k * kIntThreads + threadIdx.x;  // atom within its system
+  const uint32_t i = m.i0 + threadIdx.x, o = q.o_atom0 + off;
+  g.r[i] = g.o_r[o];
+  g.F0[i] = (q.fb0 ? g.o_F1 : g.o_F0)[o];
+  g.F1[i] = (q.fb1 ? g.o_F1 : g.o_F0)[o];
+  g.minv[i] = g.o_minv[o];
+  g.mass[i] = g.o_mass[o];
+  g.type[i] = g.o_type[o];
+  if (g.v) g.v[i] = g.o_v[o];
+  if (g.vd) {
+    // per-system planes x[n], y[n], z[n] starting at 3 x the system's first atom
+    const SysInt &S = g.sys[m.sys];
+    const size_t n = S.natoms, dst = (size_t)S.vd0 + off, src = 3 * (size_t)q.o_atom0 + off;
+    g.vd[dst] = g.o_vd[src];
+    g.vd[dst + n] = g.o_vd[src + n];
+    g.vd[dst + 2 * n] = g.o_vd[src + 2 * n];
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_fill_sysid(const BlockMap *map, uint32_t nblocks, uint32_t *sysid,
+                              cudaStream_t s) {
+  if (!nblocks) return cudaSuccess;
+  k_fill_sysid<<<nblocks, kIntThreads, 0, s>>>(map, sysid);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_state(const GatherArgs &g, cudaStream_t s) {
+  if (!g.nblocks) return cudaSuccess;
+  k_gather_state<<<g.nblocks, kIntThreads, 0, s>>>(g);
+  return cudaGetLastError();
+}
 
 uint32_t blocks_for(uint32_t natoms) { return (natoms + kIntThreads - 1) / kIntThreads; }
 

@@ -83,6 +83,34 @@ cudaError_t launch_correct_force(const IntegrateArgs &a, float4 *F, const double
 cudaError_t launch_energy_total(const double *partials, const uint32_t *item0, uint32_t nsys,
                                 DevScalars *sc, cudaStream_t s);
 
+// Owning system of every atom, written from the block map.
+cudaError_t launch_fill_sysid(const BlockMap *map, uint32_t nblocks, uint32_t *sysid,
+                              cudaStream_t s);
+
+// State of one system of a new batch that continues a system of an old one.
+struct GatherSrc {
+  int32_t src;       // old system, or -1 for a new system (left untouched)
+  uint32_t o_atom0;  // its first atom in the old arrays
+  uint8_t fb0, fb1;  // old force buffer that feeds new F[0] and new F[1]
+};
+
+struct GatherArgs {
+  const BlockMap *map;  // blocks of the new batch
+  const SysInt *sys;    // systems of the new batch
+  uint32_t nblocks;
+  const GatherSrc *gs;  // per new system
+  const float4 *o_r, *o_v, *o_F0, *o_F1;
+  const double *o_vd;
+  const float *o_minv, *o_mass;
+  const uint16_t *o_type;
+  float4 *r, *v, *F0, *F1;
+  double *vd;
+  float *minv, *mass;
+  uint16_t *type;
+};
+// Copy every continuing system's per-atom state in one launch.
+cudaError_t launch_gather_state(const GatherArgs &g, cudaStream_t s);
+
 // Host helpers: integration blocks of kIntThreads atoms aligned to each
 // system's first atom.
 uint32_t blocks_for(uint32_t natoms);
