@@ -182,6 +182,13 @@ int pb_md_adjust_velocities(pb_md *h, double v1);
 /* constTemp's force correction (cudaParticleMD.cu:140-155, correctConstTemp_F4
  * kernelfuncs.cu:533-544): F -= lambda m v on the latest force. */
 int pb_md_correct_force(pb_md *h, double lambda);
+/* initialAnnealing's pieces (cudaParticleMD.cu:205-325): the soft-core force
+ * f0 cos(pi r / 2 rc) along r for pairs inside min(rc, the LJ cutoff)
+ * (potentialSC, kernelinline.hh:136-158) on the current cell list, and the
+ * Euler step with the latest force (calcA_F4 + propagateEuler_F4 + wrap;
+ * FP32-velocity handles). */
+int pb_md_force_softcore(pb_md *h, float rc, float f0);
+int pb_md_step_euler(pb_md *h, float dt);
 /* Extension (no counterpart in the reference): steepest-descent relaxation of
  * overlapping starts, `iters` times: cell build, relaxation force (pair
  * distance floored at sigma/2 so forces stay finite), then every atom moves by

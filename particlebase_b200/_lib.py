@@ -111,6 +111,8 @@ def _declare(L: C.CDLL) -> None:
         "pb_md_correct_force": [vp, f64],
         "pb_md_set_xi": [vp, f64],
         "pb_md_minimize": [vp, u32, f32, f32],
+        "pb_md_force_softcore": [vp, f32, f32],
+        "pb_md_step_euler": [vp, f32],
         "pb_md_get": [vp, i32, vp, C.c_size_t],
         "pb_md_set": [vp, i32, vp, C.c_size_t],
         "pb_md_field_bytes": [vp, i32, C.POINTER(C.c_size_t)],

@@ -707,6 +707,28 @@ int engine_adjust(Engine &e, const double *v1) {
   return PB_OK;
 }
 
+int engine_force_softcore(Engine &e, float rc, float f0) {
+  if (!engine_ready(e)) return fail(e, PB_ERR_STATE, "need cell, LJ parameters and setup_cells");
+  if (!(rc > 0)) return fail(e, PB_ERR_ARG, "soft-core range must be > 0");
+  int nt = 1;
+  for (const auto &P : e.sp) nt = std::max(nt, P.lj.nt);
+  ForceBufs b = engine_fbufs(e);
+  b.sc_rc = rc;
+  b.sc_f0 = f0;
+  cudaError_t c = launch_force_softcore(b, nt, e.stream);
+  if (c != cudaSuccess) return cuda_fail(e, c, "soft-core force");
+  e.last = e.cur;
+  e.energy_valid = false;
+  return PB_OK;
+}
+
+int engine_euler(Engine &e, float dt) {
+  if (!e.v) return fail(e, PB_ERR_UNSUPPORTED, "the Euler step uses FP32 velocities");
+  cudaError_t c = launch_euler(engine_iargs(e, 1), e.F[e.last], dt, e.stream);
+  if (c != cudaSuccess) return cuda_fail(e, c, "Euler step");
+  return PB_OK;
+}
+
 int engine_minimize(Engine &e, uint32_t iters, float alpha, float max_disp) {
   if (!engine_ready(e)) return fail(e, PB_ERR_STATE, "need cell, LJ parameters and setup_cells");
   if (!(alpha > 0) || !(max_disp > 0)) return fail(e, PB_ERR_ARG, "alpha and max_disp must be > 0");

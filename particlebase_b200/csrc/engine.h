@@ -110,6 +110,10 @@ int engine_fv(Engine &e);
 int engine_scale(Engine &e, const double *factors);
 int engine_adjust(Engine &e, const double *v1);
 int engine_correct_force(Engine &e, const double *lambda);
+// Soft-core force (initialAnnealing) into the force buffer, cells as built.
+int engine_force_softcore(Engine &e, float rc, float f0);
+// Euler step with the latest force: r += v dt, v += F/m dt, wrap.
+int engine_euler(Engine &e, float dt);
 // Steepest-descent relaxation: iters x (cell build, relaxation force, move).
 int engine_minimize(Engine &e, uint32_t iters, float alpha, float max_disp);
 int engine_set_xi(Engine &e, const double *xi);

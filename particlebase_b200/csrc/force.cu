@@ -48,7 +48,13 @@ constexpr int kListLen = 32;    // per-lane pair list entries before a flush
 template <int NT>
 struct LJLocal {
   float s2[NT * NT], e24[NT * NT], e4[NT * NT], rc2[NT * NT], ush[NT * NT];
+  float sc_rc, sc_f0;  // soft-core mode: range and strength
 };
+
+// Pair force laws of the kernel.
+constexpr int kModeLJ = 0;        // truncated LJ (the MD step)
+constexpr int kModeCapped = 1;    // LJ with r^2 floored at (sigma/2)^2 (steepest descent)
+constexpr int kModeSoftCore = 2;  // f0 cos(pi r / 2 rc) along r (initialAnnealing)
 
 struct Stage {
   // staged index of the first atom of staged z cell k of column c (k = 0 is
@@ -64,16 +70,29 @@ struct Stage {
   int shifted;         // any nonzero frame shift in this CTA
 };
 
-// CAP: relaxation force of the steepest-descent path, with the pair distance
-// floored at sigma/2 so that overlapping random starts give finite forces.
-template <int NT, bool ENERGY, typename Acc, bool CAP = false>
+// MODE kModeCapped: relaxation force of the steepest-descent path, with the
+// pair distance floored at sigma/2 so that overlapping random starts give
+// finite forces.  MODE kModeSoftCore: the soft-core force of potentialSC
+// (kernelinline.hh:136-158) as MDpairForce applies it (kerneltemplate.hh:530-564):
+// f0 cos(r / rc * pi / 2) times the unit vector, zero beyond rc.
+template <int NT, bool ENERGY, typename Acc, int MODE = kModeLJ>
 struct PairAcc {
   Acc fx = 0, fy = 0, fz = 0, pe = 0, pes = 0, vir = 0;
   uint32_t n = 0;
   template <int M>
   __device__ __forceinline__ void add(const LJLocal<M> &lj, int k, float dx, float dy, float dz,
                                       float r2) {
-    if (CAP) r2 = fmaxf(r2, 0.25f * lj.s2[k]);
+    if (MODE == kModeSoftCore) {
+      const float r = sqrtf(r2);
+      if (r > lj.sc_rc) return;
+      const float mag = lj.sc_f0 * (float)cos((double)(r / lj.sc_rc) * 3.14159265358979323846 / 2);
+      const float f = mag * rsqrtf(r2);
+      fx += (Acc)(f * dx);
+      fy += (Acc)(f * dy);
+      fz += (Acc)(f * dz);
+      return;
+    }
+    if (MODE == kModeCapped) r2 = fmaxf(r2, 0.25f * lj.s2[k]);
     const float inv = rcp_approx(r2);
     const float sr2 = lj.s2[k] * inv;
     const float sr6 = sr2 * sr2 * sr2;
@@ -93,12 +112,12 @@ struct PairAcc {
 
 // Global-memory path (stage overflow): lanes are 32 consecutive home atoms,
 // candidates of one z cell of one column, frame shifts applied per pair.
-template <int NT, bool ENERGY, bool SELF, typename Acc, bool CAP>
+template <int NT, bool ENERGY, bool SELF, typename Acc, int MODE>
 __device__ __forceinline__ void global_range(const float4 *__restrict__ P, uint32_t jb,
                                              uint32_t je, float xi, float yi, float zi, int ti,
                                              float sx, float sy, float sz, uint32_t self,
                                              const LJLocal<NT> &lj,
-                                             PairAcc<NT, ENERGY, Acc, CAP> &a) {
+                                             PairAcc<NT, ENERGY, Acc, MODE> &a) {
   for (uint32_t j = jb; j < je; ++j) {
     const float4 q = P[j];
     const float dx = xi - (q.x - sx), dy = yi - (q.y - sy), dz = zi - (q.z - sz);
@@ -126,10 +145,10 @@ __device__ __forceinline__ uint32_t upper_bound_z(const float4 *sp, uint32_t lo,
   return lo;
 }
 
-template <int NT, bool ENERGY, typename Acc, bool CAP>
+template <int NT, bool ENERGY, typename Acc, int MODE>
 __device__ __forceinline__ void flush_list(const float4 *sp, const uint16_t *list, uint32_t cnt,
                                            int lane, float4 pi, int ti, const LJLocal<NT> &lj,
-                                           PairAcc<NT, ENERGY, Acc, CAP> &a) {
+                                           PairAcc<NT, ENERGY, Acc, MODE> &a) {
   if constexpr (NT == 1) {
     LJLocal<1> r;  // one type: parameters in registers
     r.s2[0] = lj.s2[0];
@@ -137,6 +156,8 @@ __device__ __forceinline__ void flush_list(const float4 *sp, const uint16_t *lis
     r.e4[0] = lj.e4[0];
     r.rc2[0] = lj.rc2[0];
     r.ush[0] = lj.ush[0];
+    r.sc_rc = lj.sc_rc;
+    r.sc_f0 = lj.sc_f0;
     for (uint32_t k = 0; k < cnt; ++k) {
       const float4 q = sp[list[k * 32 + lane]];
       const float dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
@@ -154,7 +175,7 @@ __device__ __forceinline__ void flush_list(const float4 *sp, const uint16_t *lis
   }
 }
 
-template <int NT, bool ENERGY, typename Acc, int kWarps, bool CAP>
+template <int NT, bool ENERGY, typename Acc, int kWarps, int MODE>
 __global__ void __launch_bounds__(kWarps * 32, 32 / kWarps) k_force(ForceBufs b) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint16_t *lists = reinterpret_cast<uint16_t *>(smem_raw);                  // kWarps*kListLen*32
@@ -184,8 +205,13 @@ __global__ void __launch_bounds__(kWarps * 32, 32 / kWarps) k_force(ForceBufs b)
     ljs.s2[threadIdx.x] = T.s2[k];
     ljs.e24[threadIdx.x] = T.e24[k];
     ljs.e4[threadIdx.x] = T.e4[k];
-    ljs.rc2[threadIdx.x] = T.rc2[k];
+    ljs.rc2[threadIdx.x] =
+        MODE == kModeSoftCore ? fminf(T.rc2[k], b.sc_rc * b.sc_rc) : T.rc2[k];
     ljs.ush[threadIdx.x] = T.ushift[k];
+  }
+  if (threadIdx.x == 0) {
+    ljs.sc_rc = b.sc_rc;
+    ljs.sc_f0 = b.sc_f0;
   }
   if (threadIdx.x < 9) {
     const int cx = it.cx, cy = it.cy;
@@ -326,7 +352,7 @@ __global__ void __launch_bounds__(kWarps * 32, 32 / kWarps) k_force(ForceBufs b)
                             : upper_bound_z(sp, lo, hi, zmax + rcw);
         }
       }
-      PairAcc<NT, ENERGY, Acc, CAP> acc;
+      PairAcc<NT, ENERGY, Acc, MODE> acc;
       uint32_t cnt = 0;
       for (int c = 0; c < 9; ++c) {
         const uint32_t jlo = __shfl_sync(0xffffffffu, bound, c);
@@ -337,7 +363,7 @@ __global__ void __launch_bounds__(kWarps * 32, 32 / kWarps) k_force(ForceBufs b)
           const uint32_t je = min(jhi, jb + 4 * kListLen);
           const uint32_t need = (je - jb + 3) >> 2;
           if (__reduce_max_sync(0xffffffffu, cnt) + need > (uint32_t)kListLen) {
-            flush_list<NT, ENERGY, Acc, CAP>(sp, mylist, cnt, lane, pi, ti, ljs, acc);
+            flush_list<NT, ENERGY, Acc, MODE>(sp, mylist, cnt, lane, pi, ti, ljs, acc);
             cnt = 0;
             __syncwarp();
           }
@@ -378,7 +404,7 @@ __global__ void __launch_bounds__(kWarps * 32, 32 / kWarps) k_force(ForceBufs b)
           cnt = (uint32_t)(out - (mylist + lane)) >> 5;
         }
       }
-      flush_list<NT, ENERGY, Acc, CAP>(sp, mylist, cnt, lane, pi, ti, ljs, acc);
+      flush_list<NT, ENERGY, Acc, MODE>(sp, mylist, cnt, lane, pi, ti, ljs, acc);
       __syncwarp();
       // combine the 4 partial sums of each home atom (lanes il, il+8, il+16, il+24)
 #pragma unroll
@@ -416,17 +442,17 @@ __global__ void __launch_bounds__(kWarps * 32, 32 / kWarps) k_force(ForceBufs b)
       const float4 p = b.rs[gh];
       const float xi = p.x - st.sx[4], yi = p.y - st.sy[4], zi = p.z - st.sz_mid;
       const int ti = NT == 1 ? 0 : __float_as_int(p.w);
-      PairAcc<NT, ENERGY, Acc, CAP> acc;
+      PairAcc<NT, ENERGY, Acc, MODE> acc;
       for (int c = 0; c < 9; ++c) {
         for (int k = kmin - 1; k <= kmax + 1; ++k) {
           const int zc = (z0 - 1 + k + nz) % nz;
           const uint32_t key = st.kbase[c] + (uint32_t)zc;
           const float sz = k == 0 ? st.sz_lo : (k == nseg + 1 ? st.sz_hi : st.sz_mid);
           if (c == 4)
-            global_range<NT, ENERGY, true, Acc, CAP>(b.rs, b.start[key], b.start[key + 1], xi, yi, zi,
+            global_range<NT, ENERGY, true, Acc, MODE>(b.rs, b.start[key], b.start[key + 1], xi, yi, zi,
                                                 ti, st.sx[c], st.sy[c], sz, gh, ljs, acc);
           else
-            global_range<NT, ENERGY, false, Acc, CAP>(b.rs, b.start[key], b.start[key + 1], xi, yi,
+            global_range<NT, ENERGY, false, Acc, MODE>(b.rs, b.start[key], b.start[key + 1], xi, yi,
                                                  zi, ti, st.sx[c], st.sy[c], sz, 0, ljs, acc);
         }
       }
@@ -453,10 +479,10 @@ __global__ void __launch_bounds__(kWarps * 32, 32 / kWarps) k_force(ForceBufs b)
   }
 }
 
-template <int NT, bool E, typename Acc, int W, bool CAP = false>
+template <int NT, bool E, typename Acc, int W, int MODE = kModeLJ>
 cudaError_t launch_w(const ForceBufs &b, cudaStream_t s) {
   const size_t smem = (size_t)W * kListLen * 32 * 2 + (size_t)b.cap * sizeof(float4);
-  auto kern = k_force<NT, E, Acc, W, CAP>;
+  auto kern = k_force<NT, E, Acc, W, MODE>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   kern<<<b.nitems, W * 32, smem, s>>>(b);
@@ -476,19 +502,28 @@ cudaError_t launch_nt(const ForceBufs &b, bool energy, bool acc64, int warps, cu
   return acc64 ? launch_t<NT, false, double>(b, warps, s) : launch_t<NT, false, float>(b, warps, s);
 }
 
+template <int MODE>
+cudaError_t launch_mode(const ForceBufs &b, int nt_max, cudaStream_t s) {
+  if (b.nitems == 0) return cudaSuccess;
+  switch (nt_max) {
+    case 1: return launch_w<1, false, float, kDefaultWarps, MODE>(b, s);
+    case 2: return launch_w<2, false, float, kDefaultWarps, MODE>(b, s);
+    case 3: case 4: return launch_w<4, false, float, kDefaultWarps, MODE>(b, s);
+    default: return launch_w<8, false, float, kDefaultWarps, MODE>(b, s);
+  }
+}
+
 }  // namespace
 
 int force_max_segment() { return kMaxSeg; }
 int force_threads() { return kDefaultWarps * 32; }
 
 cudaError_t launch_force_capped(const ForceBufs &b, int nt_max, cudaStream_t s) {
-  if (b.nitems == 0) return cudaSuccess;
-  switch (nt_max) {
-    case 1: return launch_w<1, false, float, kDefaultWarps, true>(b, s);
-    case 2: return launch_w<2, false, float, kDefaultWarps, true>(b, s);
-    case 3: case 4: return launch_w<4, false, float, kDefaultWarps, true>(b, s);
-    default: return launch_w<8, false, float, kDefaultWarps, true>(b, s);
-  }
+  return launch_mode<kModeCapped>(b, nt_max, s);
+}
+
+cudaError_t launch_force_softcore(const ForceBufs &b, int nt_max, cudaStream_t s) {
+  return launch_mode<kModeSoftCore>(b, nt_max, s);
 }
 
 cudaError_t launch_force(const ForceBufs &b, int nt_max, bool energy, bool acc64,

@@ -349,6 +349,29 @@ __global__ void __launch_bounds__(kIntThreads) k_vapply(IntegrateArgs a, const d
   }
 }
 
+// calcA_F4 + propagateEuler_F4 + applyPeriodicCondition_F4 of initialAnnealing
+// (cudaParticleMD.cu:205-325): r += v dt with the old v, then v += (F/m) dt.
+// FP32 velocities only (the annealing belongs to the plain MD class).
+__global__ void __launch_bounds__(kIntThreads) k_euler(IntegrateArgs a, const float4 *F, float dt) {
+  const BlockMap m = a.map[blockIdx.x];
+  if (threadIdx.x >= m.n) return;
+  const SysInt &S = a.sys[m.sys];
+  const uint32_t i = m.i0 + threadIdx.x;
+  const float mi = a.minv[i];
+  const float4 f = F[i];
+  float4 v = a.v[i];
+  float4 p = a.r[i];
+  p.x += v.x * dt;
+  p.y += v.y * dt;
+  p.z += v.z * dt;
+  v.x += f.x * mi * dt;
+  v.y += f.y * mi * dt;
+  v.z += f.z * mi * dt;
+  wrap3(S, p);
+  a.v[i] = v;
+  a.r[i] = p;
+}
+
 // Steepest-descent move (extension, no counterpart in the reference): each
 // atom goes along its force by F min(alpha, max_disp / |F|), then wraps.
 __global__ void __launch_bounds__(kIntThreads) k_sd_move(IntegrateArgs a, const float4 *F,
@@ -496,6 +519,10 @@ cudaError_t launch_adjust(const IntegrateArgs &a, const double *v1, cudaStream_t
   k_vstats<<<a.nblocks, kIntThreads, 0, s>>>(a);
   k_vapply<<<a.nblocks, kIntThreads, 0, s>>>(a, v1);
   return cudaGetLastError();
+}
+
+cudaError_t launch_euler(const IntegrateArgs &a, const float4 *F, float dt, cudaStream_t s) {
+  PB_LAUNCH(k_euler, a, F, dt);
 }
 
 cudaError_t launch_sd_move(const IntegrateArgs &a, const float4 *F, float alpha, float max_disp,

@@ -72,6 +72,9 @@ cudaError_t launch_fv(const IntegrateArgs &a, cudaStream_t s);
 // Per-system factors / v1 values (device arrays, one double per system).
 cudaError_t launch_scale(const IntegrateArgs &a, const double *factors, cudaStream_t s);
 cudaError_t launch_adjust(const IntegrateArgs &a, const double *v1, cudaStream_t s);
+// Euler step of initialAnnealing (calcA_F4 + propagateEuler_F4,
+// kernelfuncs.cu:70-82, 174-192): r += v dt, v += F/m dt, then wrap.
+cudaError_t launch_euler(const IntegrateArgs &a, const float4 *F, float dt, cudaStream_t s);
 // Steepest-descent move: r += F min(alpha, max_disp / |F|), then wrap.
 cudaError_t launch_sd_move(const IntegrateArgs &a, const float4 *F, float alpha, float max_disp,
                            cudaStream_t s);

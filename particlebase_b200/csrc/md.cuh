@@ -77,6 +77,7 @@ struct ForceBufs {
   double *partials;          // per-CTA energy partials (4 doubles per CTA)
   uint32_t *status;
   const uint32_t *steps_left;  // per system; 0 = finished, skipped (nullptr: all run)
+  float sc_rc, sc_f0;          // soft-core force law: range and strength
 };
 
 // Launchers (return cudaError_t of the launch).
@@ -85,5 +86,7 @@ cudaError_t launch_force(const ForceBufs &b, int nt_max, bool energy, bool acc64
                          int block_threads, cudaStream_t s);
 // Relaxation force for steepest descent: pair distance floored at sigma/2.
 cudaError_t launch_force_capped(const ForceBufs &b, int nt_max, cudaStream_t s);
+// Soft-core force f0 cos(pi r / 2 sc_rc) along r (potentialSC), for annealing.
+cudaError_t launch_force_softcore(const ForceBufs &b, int nt_max, cudaStream_t s);
 
 }  // namespace pb

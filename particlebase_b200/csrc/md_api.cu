@@ -296,6 +296,12 @@ int pb_md_correct_force(pb_md *h, double lambda) {
   return h ? engine_correct_force(h->e, &lambda) : PB_ERR_ARG;
 }
 
+int pb_md_force_softcore(pb_md *h, float rc, float f0) {
+  return h ? engine_force_softcore(h->e, rc, f0) : PB_ERR_ARG;
+}
+
+int pb_md_step_euler(pb_md *h, float dt) { return h ? engine_euler(h->e, dt) : PB_ERR_ARG; }
+
 int pb_md_minimize(pb_md *h, uint32_t iters, float alpha, float max_disp) {
   return h ? engine_minimize(h->e, iters, alpha, max_disp) : PB_ERR_ARG;
 }

@@ -20,6 +20,8 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <memory>
@@ -77,6 +79,7 @@ struct pb_srv {
   std::vector<Job *> slots;  // job of each batch system
   double ms_per_atom_step = 5e-7;
   double last_repack_ms = 0.0;
+  bool trace = false;  // PB_SRV_TRACE: per-repack phase times on stderr
   std::thread worker;
 
   double now() const {
@@ -230,6 +233,13 @@ void scheduler(pb_srv *s) {
       }
       pb_batch *nb = nullptr;
       int rc;
+      auto lap = [t = std::chrono::steady_clock::now()]() mutable {
+        const auto n = std::chrono::steady_clock::now();
+        const double ms = std::chrono::duration<double, std::milli>(n - t).count();
+        t = n;
+        return ms;
+      };
+      double ph[5] = {0, 0, 0, 0, 0};
       if (s->batch && !keep.empty()) {
         rc = pb_batch_repack(s->batch, src.data(), nat.data(), nsys, &nb);
       } else {
@@ -240,19 +250,33 @@ void scheduler(pb_srv *s) {
       }
       std::string why = rc ? std::string("repack: ") + (s->batch ? pb_batch_last_error(s->batch) : "")
                            : std::string();
+      ph[0] = lap();
       for (uint32_t a = 0; a < admit.size() && !rc; ++a) {
         rc = setup_new(nb, (uint32_t)keep.size() + a, *admit[a]);
         if (rc) why = std::string("admit: ") + pb_batch_last_error(nb);
       }
+      ph[1] = lap();
       if (!rc) {
         rc = pb_batch_setup_cells(nb, nullptr);
         if (rc) why = std::string("setup_cells: ") + pb_batch_last_error(nb);
       }
+      ph[2] = lap();
       std::vector<uint32_t> rem(nsys);
       for (uint32_t k = 0; k < nsys; ++k) rem[k] = slots[k]->remaining;
       if (!rc) rc = pb_batch_set_steps_left(nb, rem.data());
+      ph[3] = lap();
       if (s->batch) pb_batch_destroy(s->batch);
       s->batch = nb;
+      ph[4] = lap();
+      if (s->trace) {
+        uint64_t natoms = 0;
+        for (Job *j : slots) natoms += j->n;
+        std::fprintf(stderr,
+                     "pb_srv repack: %u jobs (%zu kept, %zu new, %zu done), %llu atoms; ms: "
+                     "repack %.2f admit %.2f cells %.2f budgets %.2f free %.2f\n",
+                     nsys, keep.size(), admit.size(), done.size(), (unsigned long long)natoms,
+                     ph[0], ph[1], ph[2], ph[3], ph[4]);
+      }
       {
         std::lock_guard<std::mutex> lk(s->mu);
         s->slots = slots;
@@ -336,6 +360,7 @@ int pb_srv_create(const pb_srv_config *cfg, pb_srv **out) {
     }
     s->budget = (size_t)(0.9 * (double)fr);
   }
+  if (const char *t = std::getenv("PB_SRV_TRACE")) s->trace = t[0] && t[0] != '0';
   s->worker = std::thread(scheduler, s);
   *out = s;
   return PB_OK;

@@ -131,10 +131,37 @@ class cudaParticleMD : public cudaParticleVV,
     pb_shim::check(pb_md_set_lj(h, q.data(), elemnum), "setLJparams", h);
   }
 
-  // Soft-core annealing (cudaParticleMD.cu:205-325) is not provided.
-  void initialAnnealing(uint32_t, real, real, real, real) {
-    std::cerr << "particlebase_b200: initialAnnealing is not provided by this library" << std::endl;
-    std::exit(1);
+  // cudaParticleMD::initialAnnealing (cudaParticleMD.cu:205-325): anealstep
+  // Euler steps under a soft-core repulsion whose range grows to _rc, each
+  // with the constTemp force correction, a temperature rescale, then anealstep
+  // velocity-Verlet LJ steps with constTemp, and a final rescale.
+  void initialAnnealing(uint32_t anealstep, real dt, real _rc, real _f0, real T) {
+    need("initialAnnealing");
+    sync_params();
+    std::cerr << "performs initial annealing by soft core potential to rmax= " << _rc
+              << " with steps " << anealstep << std::endl;
+    for (uint32_t i = 0; i < anealstep; ++i) {
+      const real rc = _rc * (i + 1) / anealstep;
+      std::cerr << "\r" << rc << "\t" << std::flush;
+      calcBlockID();
+      pb_shim::check(pb_md_force_softcore(h, rc, _f0), "initialAnnealing", h);
+      constTemp();
+      pb_shim::check(pb_md_step_euler(h, dt), "initialAnnealing", h);
+      std::cerr << "T= " << calcTemp() << std::flush;
+    }
+    std::cerr << std::endl;
+    std::cerr << "temperature scaling: " << scaleTemp(T) << std::endl;
+    std::cerr << "with LJ " << std::endl;
+    clearForce();  // Fold = 0 before the LJ stage
+    for (uint32_t i = 0; i < anealstep; ++i) {
+      std::cerr << i << "\t" << calcTemp() << "\t";
+      calcBlockID();
+      calcForce();
+      std::cerr << constTemp() << std::endl;
+      pb_shim::check(pb_md_step_vv(h, dt), "initialAnnealing", h);
+      treatPeriodicCondition();
+    }
+    std::cerr << "temperature scaling: " << scaleTemp(T) << std::endl;
   }
 
   // per-particle m v^2, one line each (cudaParticleMD.cu:157-166)

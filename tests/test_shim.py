@@ -86,3 +86,27 @@ def test_testMD2_runs_on_the_drop_in_classes(cuda_lib, tmp_path):
     assert d2[0][0] == 16000 and d2[-1][0] == 32000
     # the first frame after the restart is the last frame before it
     assert np.array_equal(d2[0][3], dumps[-1][3])
+
+
+@pytest.mark.gpu
+def test_testMD1_with_soft_core_annealing(cuda_lib, tmp_path):
+    """testMD1: initialAnnealing (soft-core Euler stage, then LJ velocity
+    Verlet, each with the constTemp correction) followed by 20,000 NVE steps
+    with temperature rescaling, run unchanged on the drop-in classes."""
+    exe = os.path.join(DRIVERS, "testMD1")
+    if not os.path.exists(exe):
+        pytest.skip("drivers not built (reference checkout absent at build time)")
+    out = tmp_path / "dump.txt"
+    err = tmp_path / "log.txt"
+    with open(out, "w") as fo, open(err, "w") as fe:
+        r = subprocess.run([exe], cwd=tmp_path, stdout=fo, stderr=fe, timeout=900)
+    log = err.read_text()
+    assert r.returncode == 0, log[-2000:]
+    assert "abort" not in log
+    assert "performs initial annealing by soft core potential" in log
+    assert log.count("temperature scaling:") == 2
+    dumps = _parse_dumps(out.read_text())
+    n = dumps[0][1]
+    assert len(dumps) >= 100 and all(d[1] == n for d in dumps)
+    for ts, n, box, atoms in dumps:
+        assert np.isfinite(atoms).all()
