@@ -282,7 +282,8 @@ int pb_batch_set_lj_cut(pb_batch *b, uint32_t sys, const float *sigma_eps_rc, ui
 int pb_batch_import(pb_batch *b, uint32_t sys, const double *r3, const double *v3,
                     const double *mass, const uint32_t *type);
 /* Cell grids of all systems; rmax[sys] per system, or NULL for each system's
- * LJ cutoff. */
+ * LJ cutoff.  Also uploads the parameters given to pb_batch_set_system and
+ * pb_batch_set_lj_cut since the last setup (they take effect here). */
 int pb_batch_setup_cells(pb_batch *b, const float *rmax);
 /* Cell build + force for all systems (pb_md_build_cells + pb_md_force). */
 int pb_batch_force(pb_batch *b, uint32_t flags);

@@ -229,10 +229,9 @@ int pb_batch_set_system(pb_batch *b, uint32_t sys, const float cell6[6], float r
   lj_table_fill(P, sigma_eps, ntypes, 2, false);
   P.dt = dt;
   P.kB = kB;
-  b->e.cells_ready = false;
+  b->e.cells_ready = false;  // pb_batch_setup_cells uploads the tables of all systems
   engine_drop_graph(b->e);
-  const int r = engine_upload_lj(b->e);
-  return r ? r : engine_upload_sysint(b->e);
+  return PB_OK;
 }
 
 int pb_batch_set_lj_cut(pb_batch *b, uint32_t sys, const float *p, uint32_t ntypes) {
@@ -245,9 +244,9 @@ int pb_batch_set_lj_cut(pb_batch *b, uint32_t sys, const float *p, uint32_t ntyp
   for (uint32_t k = 0; k < ntypes * ntypes; ++k) rc2 = std::max(rc2, P.lj.rc2[k]);
   P.rmax2 = rc2;
   P.rmax = std::sqrt(rc2);
-  b->e.cells_ready = false;
+  b->e.cells_ready = false;  // uploaded by pb_batch_setup_cells
   engine_drop_graph(b->e);
-  return engine_upload_lj(b->e);
+  return PB_OK;
 }
 
 int pb_batch_import(pb_batch *b, uint32_t sys, const double *r3, const double *v3,

@@ -30,10 +30,10 @@ int cuda_fail(Engine &e, cudaError_t c, const char *what) {
     if (c_ != cudaSuccess) return cuda_fail(e, c_, #call); \
   } while (0)
 
-// Engine memory comes from a stream-ordered pool per device that keeps up to
-// kPoolKeep bytes of freed memory, so the batches a server builds and drops at
-// every repack reuse memory instead of going back to the driver.
-constexpr uint64_t kPoolKeep = 8ull << 30;
+// Engine memory comes from a stream-ordered pool per device that keeps the
+// memory it frees (a caching allocator), so the batches a server builds and
+// drops at every repack reuse memory instead of mapping new pages each time.
+constexpr uint64_t kPoolKeep = ~0ull;
 
 cudaMemPool_t device_pool() {
   static std::mutex mu;
@@ -431,7 +431,9 @@ int engine_setup_cells(Engine &e) {
   E_CUDA(cudaMemcpyAsync(e.d_item0, e.item0.data(), 4 * (size_t)(e.nsys + 1),
                          cudaMemcpyHostToDevice, e.stream));
   E_CUDA(cudaStreamSynchronize(e.stream));
-  int rc = engine_upload_sysint(e);
+  int rc = engine_upload_lj(e);  // parameters set since the last upload
+  if (rc) return rc;
+  rc = engine_upload_sysint(e);
   if (rc) return rc;
   e.cells_ready = true;
   return PB_OK;
