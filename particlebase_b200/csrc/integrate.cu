@@ -114,8 +114,8 @@ __global__ void __launch_bounds__(kIntThreads) k_vv(IntegrateArgs a) {
   if (finished(a, m.sys)) return;
   const SysInt &S = a.sys[m.sys];
   double mv2 = 0;
-  if (threadIdx.x < m.n) {
-    const uint32_t i = m.i0 + threadIdx.x;
+  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
+    const uint32_t i = m.i0 + t;
     const float dt = S.dt;
     const float dt2 = dt * 0.5f;
     const float h = dt2 * a.minv[i];  // dt / 2m
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(kIntThreads) k_vv(IntegrateArgs a) {
     if (a.wrap) wrap3(S, p);
     a.v[i] = v;
     a.r[i] = p;
-    mv2 = (double)a.mass[i] * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+    mv2 += (double)a.mass[i] * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
   }
   double s[1] = {mv2}, tot[1];
   block_sum<1>(s, red);
@@ -166,13 +166,13 @@ __global__ void __launch_bounds__(kIntThreads) k_gauss_a(IntegrateArgs a) {
   DevScalars &sc = a.sc[m.sys];
   const double xi_old = sc.xi_old;
   double s[2] = {0, 0};
-  if (threadIdx.x < m.n) {
-    const uint32_t i = m.i0 + threadIdx.x;
+  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
+    const uint32_t i = m.i0 + t;
     double A[3];
     float4 F;
     gauss_A(a, S, i, xi_old, A, F);
-    s[0] = (double)F.x * A[0] + (double)F.y * A[1] + (double)F.z * A[2];
-    s[1] = (double)a.mass[i] * (A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+    s[0] += (double)F.x * A[0] + (double)F.y * A[1] + (double)F.z * A[2];
+    s[1] += (double)a.mass[i] * (A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
   }
   double tot[2];
   block_sum<2>(s, red);
@@ -199,8 +199,8 @@ __global__ void __launch_bounds__(kIntThreads) k_gauss_b(IntegrateArgs a) {
   const double xi_old = sc.xi_old;
   const double xi = sc.xi_new;
   double mv2 = 0;
-  if (threadIdx.x < m.n) {
-    const uint32_t i = m.i0 + threadIdx.x;
+  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
+    const uint32_t i = m.i0 + t;
     double A[3];
     float4 F;
     gauss_A(a, S, i, xi_old, A, F);
@@ -217,11 +217,11 @@ __global__ void __launch_bounds__(kIntThreads) k_gauss_b(IntegrateArgs a) {
     a.r[i] = p;
     if (a.vd) {
       store_vd(a, S, i, v);
-      mv2 = (double)a.mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      mv2 += (double)a.mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
     } else {
       const float4 vf = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
       a.v[i] = vf;
-      mv2 = (double)a.mass[i] * ((double)vf.x * vf.x + (double)vf.y * vf.y + (double)vf.z * vf.z);
+      mv2 += (double)a.mass[i] * ((double)vf.x * vf.x + (double)vf.y * vf.y + (double)vf.z * vf.z);
     }
   }
   double s[1] = {mv2}, tot[1];
@@ -236,11 +236,12 @@ __global__ void __launch_bounds__(kIntThreads) k_gauss_b(IntegrateArgs a) {
 
 __global__ void __launch_bounds__(kIntThreads) k_wrap(IntegrateArgs a) {
   const BlockMap m = a.map[blockIdx.x];
-  if (threadIdx.x >= m.n) return;
-  const uint32_t i = m.i0 + threadIdx.x;
-  float4 p = a.r[i];
-  wrap3(a.sys[m.sys], p);
-  a.r[i] = p;
+  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
+    const uint32_t i = m.i0 + t;
+    float4 p = a.r[i];
+    wrap3(a.sys[m.sys], p);
+    a.r[i] = p;
+  }
 }
 
 __global__ void __launch_bounds__(kIntThreads) k_mv2(IntegrateArgs a) {
@@ -248,11 +249,11 @@ __global__ void __launch_bounds__(kIntThreads) k_mv2(IntegrateArgs a) {
   const BlockMap m = a.map[blockIdx.x];
   const SysInt &S = a.sys[m.sys];
   double s[1] = {0};
-  if (threadIdx.x < m.n) {
-    const uint32_t i = m.i0 + threadIdx.x;
+  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
+    const uint32_t i = m.i0 + t;
     double v[3];
     load_v(a, S, i, v);
-    s[0] = (double)a.mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    s[0] += (double)a.mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
   }
   double tot[1];
   block_sum<1>(s, red);
@@ -265,12 +266,12 @@ __global__ void __launch_bounds__(kIntThreads) k_fv(IntegrateArgs a) {
   const BlockMap m = a.map[blockIdx.x];
   const SysInt &S = a.sys[m.sys];
   double s[1] = {0};
-  if (threadIdx.x < m.n) {
-    const uint32_t i = m.i0 + threadIdx.x;
+  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
+    const uint32_t i = m.i0 + t;
     const float4 F = a.F[i];
     double v[3];
     load_v(a, S, i, v);
-    s[0] = (double)F.x * v[0] + (double)F.y * v[1] + (double)F.z * v[2];
+    s[0] += (double)F.x * v[0] + (double)F.y * v[1] + (double)F.z * v[2];
   }
   double tot[1];
   block_sum<1>(s, red);
@@ -280,23 +281,24 @@ __global__ void __launch_bounds__(kIntThreads) k_fv(IntegrateArgs a) {
 
 __global__ void __launch_bounds__(kIntThreads) k_scale(IntegrateArgs a, const double *f) {
   const BlockMap m = a.map[blockIdx.x];
-  if (threadIdx.x >= m.n) return;
-  const SysInt &S = a.sys[m.sys];
-  const uint32_t i = m.i0 + threadIdx.x;
-  const double s = f[m.sys];
-  if (a.vd) {
-    double v[3];
-    load_vd(a, S, i, v);
-    for (int k = 0; k < 3; ++k) v[k] *= s;
-    store_vd(a, S, i, v);
-  } else {
-    const float sf = (float)s;
-    float4 v = a.v[i];
-    v.x *= sf;
-    v.y *= sf;
-    v.z *= sf;
-    v.w *= sf;
-    a.v[i] = v;
+  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
+    const SysInt &S = a.sys[m.sys];
+    const uint32_t i = m.i0 + t;
+    const double s = f[m.sys];
+    if (a.vd) {
+      double v[3];
+      load_vd(a, S, i, v);
+      for (int k = 0; k < 3; ++k) v[k] *= s;
+      store_vd(a, S, i, v);
+    } else {
+      const float sf = (float)s;
+      float4 v = a.v[i];
+      v.x *= sf;
+      v.y *= sf;
+      v.z *= sf;
+      v.w *= sf;
+      a.v[i] = v;
+    }
   }
 }
 
@@ -307,12 +309,12 @@ __global__ void __launch_bounds__(kIntThreads) k_vstats(IntegrateArgs a) {
   const BlockMap m = a.map[blockIdx.x];
   const SysInt &S = a.sys[m.sys];
   double s[6] = {0, 0, 0, 0, 0, 0};
-  if (threadIdx.x < m.n) {
+  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
     double w[3];
-    load_v(a, S, m.i0 + threadIdx.x, w);
+    load_v(a, S, m.i0 + t, w);
     for (int k = 0; k < 3; ++k) {
-      s[k] = w[k];
-      s[3 + k] = w[k] * w[k];
+      s[k] += w[k];
+      s[3 + k] += w[k] * w[k];
     }
   }
   double tot[6];
@@ -324,28 +326,29 @@ __global__ void __launch_bounds__(kIntThreads) k_vstats(IntegrateArgs a) {
 
 __global__ void __launch_bounds__(kIntThreads) k_vapply(IntegrateArgs a, const double *v1s) {
   const BlockMap m = a.map[blockIdx.x];
-  if (threadIdx.x >= m.n) return;
-  const SysInt &S = a.sys[m.sys];
-  const uint32_t i = m.i0 + threadIdx.x;
-  const DevScalars &sc = a.sc[m.sys];
-  const double n = (double)S.natoms, v1 = v1s[m.sys];
-  double mean[3], f[3];
-  for (int k = 0; k < 3; ++k) {
-    mean[k] = sc.vstat[k] / n;
-    const double var = sc.vstat[3 + k] / n - mean[k] * mean[k];
-    f[k] = var > 0 ? v1 / sqrt(var) : 0.0;
-  }
-  if (a.vd) {
-    double v[3];
-    load_vd(a, S, i, v);
-    for (int k = 0; k < 3; ++k) v[k] = (v[k] - mean[k]) * f[k];
-    store_vd(a, S, i, v);
-  } else {
-    float4 v = a.v[i];
-    v.x = (float)((v.x - mean[0]) * f[0]);
-    v.y = (float)((v.y - mean[1]) * f[1]);
-    v.z = (float)((v.z - mean[2]) * f[2]);
-    a.v[i] = v;
+  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
+    const SysInt &S = a.sys[m.sys];
+    const uint32_t i = m.i0 + t;
+    const DevScalars &sc = a.sc[m.sys];
+    const double n = (double)S.natoms, v1 = v1s[m.sys];
+    double mean[3], f[3];
+    for (int k = 0; k < 3; ++k) {
+      mean[k] = sc.vstat[k] / n;
+      const double var = sc.vstat[3 + k] / n - mean[k] * mean[k];
+      f[k] = var > 0 ? v1 / sqrt(var) : 0.0;
+    }
+    if (a.vd) {
+      double v[3];
+      load_vd(a, S, i, v);
+      for (int k = 0; k < 3; ++k) v[k] = (v[k] - mean[k]) * f[k];
+      store_vd(a, S, i, v);
+    } else {
+      float4 v = a.v[i];
+      v.x = (float)((v.x - mean[0]) * f[0]);
+      v.y = (float)((v.y - mean[1]) * f[1]);
+      v.z = (float)((v.z - mean[2]) * f[2]);
+      a.v[i] = v;
+    }
   }
 }
 
@@ -354,22 +357,23 @@ __global__ void __launch_bounds__(kIntThreads) k_vapply(IntegrateArgs a, const d
 // FP32 velocities only (the annealing belongs to the plain MD class).
 __global__ void __launch_bounds__(kIntThreads) k_euler(IntegrateArgs a, const float4 *F, float dt) {
   const BlockMap m = a.map[blockIdx.x];
-  if (threadIdx.x >= m.n) return;
-  const SysInt &S = a.sys[m.sys];
-  const uint32_t i = m.i0 + threadIdx.x;
-  const float mi = a.minv[i];
-  const float4 f = F[i];
-  float4 v = a.v[i];
-  float4 p = a.r[i];
-  p.x += v.x * dt;
-  p.y += v.y * dt;
-  p.z += v.z * dt;
-  v.x += f.x * mi * dt;
-  v.y += f.y * mi * dt;
-  v.z += f.z * mi * dt;
-  wrap3(S, p);
-  a.v[i] = v;
-  a.r[i] = p;
+  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
+    const SysInt &S = a.sys[m.sys];
+    const uint32_t i = m.i0 + t;
+    const float mi = a.minv[i];
+    const float4 f = F[i];
+    float4 v = a.v[i];
+    float4 p = a.r[i];
+    p.x += v.x * dt;
+    p.y += v.y * dt;
+    p.z += v.z * dt;
+    v.x += f.x * mi * dt;
+    v.y += f.y * mi * dt;
+    v.z += f.z * mi * dt;
+    wrap3(S, p);
+    a.v[i] = v;
+    a.r[i] = p;
+  }
 }
 
 // Steepest-descent move (extension, no counterpart in the reference): each
@@ -377,36 +381,38 @@ __global__ void __launch_bounds__(kIntThreads) k_euler(IntegrateArgs a, const fl
 __global__ void __launch_bounds__(kIntThreads) k_sd_move(IntegrateArgs a, const float4 *F,
                                                         float alpha, float max_disp) {
   const BlockMap m = a.map[blockIdx.x];
-  if (threadIdx.x >= m.n) return;
-  const SysInt &S = a.sys[m.sys];
-  const uint32_t i = m.i0 + threadIdx.x;
-  const float4 f = F[i];
-  const float fn = sqrtf(fmaf(f.x, f.x, fmaf(f.y, f.y, f.z * f.z)));
-  const float g = fn * alpha > max_disp ? max_disp / fn : alpha;
-  float4 p = a.r[i];
-  p.x = fmaf(g, f.x, p.x);
-  p.y = fmaf(g, f.y, p.y);
-  p.z = fmaf(g, f.z, p.z);
-  wrap3(S, p);
-  a.r[i] = p;
+  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
+    const SysInt &S = a.sys[m.sys];
+    const uint32_t i = m.i0 + t;
+    const float4 f = F[i];
+    const float fn = sqrtf(fmaf(f.x, f.x, fmaf(f.y, f.y, f.z * f.z)));
+    const float g = fn * alpha > max_disp ? max_disp / fn : alpha;
+    float4 p = a.r[i];
+    p.x = fmaf(g, f.x, p.x);
+    p.y = fmaf(g, f.y, p.y);
+    p.z = fmaf(g, f.z, p.z);
+    wrap3(S, p);
+    a.r[i] = p;
+  }
 }
 
 // correctConstTemp_F4 (kernelfuncs.cu:533-544): F -= lambda m v, per system.
 __global__ void __launch_bounds__(kIntThreads) k_correct(IntegrateArgs a, float4 *F,
                                                         const double *lambda) {
   const BlockMap m = a.map[blockIdx.x];
-  if (threadIdx.x >= m.n) return;
-  const SysInt &S = a.sys[m.sys];
-  const uint32_t i = m.i0 + threadIdx.x;
-  double v[3];
-  load_v(a, S, i, v);
-  const float l = (float)lambda[m.sys];
-  const float mi = a.mass[i];
-  float4 f = F[i];
-  f.x -= l * mi * (float)v[0];
-  f.y -= l * mi * (float)v[1];
-  f.z -= l * mi * (float)v[2];
-  F[i] = f;
+  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
+    const SysInt &S = a.sys[m.sys];
+    const uint32_t i = m.i0 + t;
+    double v[3];
+    load_v(a, S, i, v);
+    const float l = (float)lambda[m.sys];
+    const float mi = a.mass[i];
+    float4 f = F[i];
+    f.x -= l * mi * (float)v[0];
+    f.y -= l * mi * (float)v[1];
+    f.z -= l * mi * (float)v[2];
+    F[i] = f;
+  }
 }
 
 // One block per system: energy partials of the system's force items, in order.
@@ -434,29 +440,31 @@ __global__ void __launch_bounds__(kIntThreads) k_energy_total(const double *part
 
 __global__ void __launch_bounds__(kIntThreads) k_fill_sysid(const BlockMap *map, uint32_t *sysid) {
   const BlockMap m = map[blockIdx.x];
-  if (threadIdx.x < m.n) sysid[m.i0 + threadIdx.x] = m.sys;
+  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) sysid[m.i0 + t] = m.sys;
 }
 
 __global__ void __launch_bounds__(kIntThreads) k_gather_state(GatherArgs g) {
   const BlockMap m = g.map[blockIdx.x];
   const GatherSrc q = g.gs[m.sys];
-  if (q.src < 0 || threadIdx.x >= m.n) return;
-  const uint32_t off = m.k * kIntThreads + threadIdx.x;  // atom within its system
-  const uint32_t i = m.i0 + threadIdx.x, o = q.o_atom0 + off;
-  g.r[i] = g.o_r[o];
-  g.F0[i] = (q.fb0 ? g.o_F1 : g.o_F0)[o];
-  g.F1[i] = (q.fb1 ? g.o_F1 : g.o_F0)[o];
-  g.minv[i] = g.o_minv[o];
-  g.mass[i] = g.o_mass[o];
-  g.type[i] = g.o_type[o];
-  if (g.v) g.v[i] = g.o_v[o];
-  if (g.vd) {
-    // per-system planes x[n], y[n], z[n] starting at 3 x the system's first atom
-    const SysInt &S = g.sys[m.sys];
-    const size_t n = S.natoms, dst = (size_t)S.vd0 + off, src = 3 * (size_t)q.o_atom0 + off;
-    g.vd[dst] = g.o_vd[src];
-    g.vd[dst + n] = g.o_vd[src + n];
-    g.vd[dst + 2 * n] = g.o_vd[src + 2 * n];
+  if (q.src < 0) return;
+  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
+    const uint32_t off = m.k * kIntAtoms + t;  // atom within its system
+    const uint32_t i = m.i0 + t, o = q.o_atom0 + off;
+    g.r[i] = g.o_r[o];
+    g.F0[i] = (q.fb0 ? g.o_F1 : g.o_F0)[o];
+    g.F1[i] = (q.fb1 ? g.o_F1 : g.o_F0)[o];
+    g.minv[i] = g.o_minv[o];
+    g.mass[i] = g.o_mass[o];
+    g.type[i] = g.o_type[o];
+    if (g.v) g.v[i] = g.o_v[o];
+    if (g.vd) {
+      // per-system planes x[n], y[n], z[n] starting at 3 x the system's first atom
+      const SysInt &S = g.sys[m.sys];
+      const size_t n = S.natoms, dst = (size_t)S.vd0 + off, src = 3 * (size_t)q.o_atom0 + off;
+      g.vd[dst] = g.o_vd[src];
+      g.vd[dst + n] = g.o_vd[src + n];
+      g.vd[dst + 2 * n] = g.o_vd[src + 2 * n];
+    }
   }
 }
 
@@ -475,7 +483,7 @@ cudaError_t launch_gather_state(const GatherArgs &g, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-uint32_t blocks_for(uint32_t natoms) { return (natoms + kIntThreads - 1) / kIntThreads; }
+uint32_t blocks_for(uint32_t natoms) { return (natoms + kIntAtoms - 1) / kIntAtoms; }
 
 void make_block_map(const uint32_t *natoms, uint32_t nsys, BlockMap *map, uint32_t *blk0,
                     uint32_t *nblk) {
@@ -484,9 +492,9 @@ void make_block_map(const uint32_t *natoms, uint32_t nsys, BlockMap *map, uint32
     blk0[s] = b;
     nblk[s] = blocks_for(natoms[s]);
     for (uint32_t k = 0; k < nblk[s]; ++k) {
-      const uint32_t i0 = atom0 + k * kIntThreads;
-      const uint32_t n = natoms[s] - k * kIntThreads;
-      map[b++] = BlockMap{s, i0, n < (uint32_t)kIntThreads ? n : (uint32_t)kIntThreads, k};
+      const uint32_t i0 = atom0 + k * kIntAtoms;
+      const uint32_t n = natoms[s] - k * kIntAtoms;
+      map[b++] = BlockMap{s, i0, n < (uint32_t)kIntAtoms ? n : (uint32_t)kIntAtoms, k};
     }
     atom0 += natoms[s];
   }

@@ -12,7 +12,8 @@
 
 namespace pb {
 
-constexpr int kIntThreads = 256;  // atoms per integration block
+constexpr int kIntThreads = 256;  // threads per integration block
+constexpr int kIntAtoms = 1024;   // atoms per integration block (4 per thread, strided)
 
 // Device-resident scalars of one system.  Reductions are finished on the
 // device (last-block pattern), so a step never needs a host round trip.
@@ -38,8 +39,8 @@ struct SysInt {
   float c0[3], c1[3], L[3];  // box for the wrap
 };
 
-// Block b of an integration launch covers atoms [i0, i0 + n) of system sys;
-// it is block `k` of that system.
+// Block b of an integration launch covers atoms [i0, i0 + n) of system sys,
+// n <= kIntAtoms; it is block `k` of that system (i0 = first atom + k kIntAtoms).
 struct BlockMap {
   uint32_t sys, i0, n, k;
 };
@@ -114,7 +115,7 @@ struct GatherArgs {
 // Copy every continuing system's per-atom state in one launch.
 cudaError_t launch_gather_state(const GatherArgs &g, cudaStream_t s);
 
-// Host helpers: integration blocks of kIntThreads atoms aligned to each
+// Host helpers: integration blocks of kIntAtoms atoms aligned to each
 // system's first atom.
 uint32_t blocks_for(uint32_t natoms);
 void make_block_map(const uint32_t *natoms, uint32_t nsys, BlockMap *map, uint32_t *blk0,
