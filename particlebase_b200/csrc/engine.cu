@@ -124,6 +124,10 @@ void free_cells(Engine &e) {
 void engine_drop_graph(Engine &e) {
   if (e.graph) cudaGraphExecDestroy(e.graph);
   e.graph = nullptr;
+  for (auto &g : e.graph1) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
   e.graph_mode = -1;
   e.graph_dt.clear();
 }
@@ -564,33 +568,39 @@ int engine_run(Engine &e, int mode, uint32_t steps) {
   if (mode == PB_MODE_VV && e.vd) return fail(e, PB_ERR_UNSUPPORTED, "VV needs FP32 velocities");
   std::vector<float> dts(e.nsys);
   for (uint32_t s = 0; s < e.nsys; ++s) dts[s] = e.sp[s].dt;
+  if (e.graph_mode != mode || e.graph_dt != dts) engine_drop_graph(e);
+  e.graph_mode = mode;
+  e.graph_dt = dts;
+  // capture `n` whole steps starting from the current ping-pong parity
+  auto capture = [&](int n, cudaGraphExec_t *out) -> int {
+    cudaGraph_t g = nullptr;
+    const int cur0 = e.cur, last0 = e.last;
+    const uint64_t done0 = e.steps_done;
+    E_CUDA(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
+    int rc = PB_OK;
+    for (int k = 0; k < n && !rc; ++k) rc = engine_step(e, mode);
+    cudaError_t c = cudaStreamEndCapture(e.stream, &g);
+    e.cur = cur0;  // the captured steps have not run yet
+    e.last = last0;
+    e.steps_done = done0;
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (c != cudaSuccess) return cuda_fail(e, c, "graph capture");
+    c = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (c != cudaSuccess) {
+      *out = nullptr;
+      return cuda_fail(e, c, "graph instantiate");
+    }
+    return PB_OK;
+  };
   uint32_t done = 0;
   if (steps >= 2) {
-    if (!e.graph || e.graph_mode != mode || e.graph_dt != dts) {
-      engine_drop_graph(e);
-      cudaGraph_t g = nullptr;
-      const int cur0 = e.cur, last0 = e.last;
-      const uint64_t done0 = e.steps_done;
-      E_CUDA(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
-      int rc = engine_step(e, mode);
-      if (!rc) rc = engine_step(e, mode);
-      cudaError_t c = cudaStreamEndCapture(e.stream, &g);
-      e.cur = cur0;  // the captured steps have not run yet
-      e.last = last0;
-      e.steps_done = done0;
-      if (rc) {
-        if (g) cudaGraphDestroy(g);
-        return rc;
-      }
-      if (c != cudaSuccess) return cuda_fail(e, c, "graph capture");
-      c = cudaGraphInstantiate(&e.graph, g, 0);
-      cudaGraphDestroy(g);
-      if (c != cudaSuccess) {
-        e.graph = nullptr;
-        return cuda_fail(e, c, "graph instantiate");
-      }
-      e.graph_mode = mode;
-      e.graph_dt = dts;
+    if (!e.graph) {
+      const int rc = capture(2, &e.graph);
+      if (rc) return rc;
     }
     for (; done + 2 <= steps; done += 2) {
       E_CUDA(cudaGraphLaunch(e.graph, e.stream));
@@ -598,9 +608,16 @@ int engine_run(Engine &e, int mode, uint32_t steps) {
       e.last = 1 - e.cur;  // two steps: cur is back where it was, F[1 - cur] is the newest
     }
   }
-  for (; done < steps; ++done) {
-    int rc = engine_step(e, mode);
-    if (rc) return rc;
+  if (done < steps) {  // one step left: the one-step graph of this parity
+    cudaGraphExec_t &g1 = e.graph1[e.cur];
+    if (!g1) {
+      const int rc = capture(1, &g1);
+      if (rc) return rc;
+    }
+    E_CUDA(cudaGraphLaunch(g1, e.stream));
+    e.steps_done += 1;
+    e.last = e.cur;
+    e.cur = 1 - e.cur;
   }
   e.energy_valid = false;
   return PB_OK;

@@ -80,8 +80,10 @@ struct Engine {
   std::vector<uint64_t> budget_end;  // steps_done at which each budget runs out
   std::vector<int> last_at_set;      // `last` when each budget was set
 
-  // CUDA graph of two whole steps (the F ping-pong returns to its parity)
+  // CUDA graph of two whole steps (the F ping-pong returns to its parity), and
+  // one-step graphs for each parity of the ping-pong
   cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph1[2] = {nullptr, nullptr};
   int graph_mode = -1;
   std::vector<float> graph_dt;
 };
