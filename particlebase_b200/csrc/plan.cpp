@@ -80,7 +80,8 @@ int choose_capacity(double atoms_per_cell, int seg) {
   double factor = 1.15;  // headroom over the mean occupancy; PB_FORCE_CAP overrides
   if (const char *e = std::getenv("PB_FORCE_CAP")) factor = std::atof(e);
   const double cap = factor * expect + 128.0;
-  const double max_atoms = (190.0 * 1024.0) / 16.0;
+  // the largest launch shape (8 warps, 8 types) bounds every launch's memory
+  const double max_atoms = (double)force_max_capacity(8, kMaxTypes);
   return (int)std::min(cap, max_atoms);
 }
 

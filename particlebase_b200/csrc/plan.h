@@ -39,5 +39,7 @@ void append_items(uint32_t sys, const Grid &g, int seg, uint32_t cell0,
                   std::vector<ForceItem> &items);
 
 int force_max_segment();
+// Largest staged-atom capacity of a force CTA of `warps` warps for `nt` types.
+int force_max_capacity(int warps, int nt);
 
 }  // namespace pb
