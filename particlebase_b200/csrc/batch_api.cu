@@ -400,8 +400,9 @@ int pb_batch_estimate_bytes(const uint32_t *natoms, const float *cells6, const f
                             uint32_t nsys, uint32_t flags, size_t *bytes) {
   if (!natoms || !cells6 || !rmax || !bytes || nsys == 0) return PB_ERR_ARG;
   // per atom: r, F[2], rs (16 B each), minv, mass, key, within, pid_tmp, pid,
-  // slot (4 B each), type (2 B), velocities (16 or 24 B), sysid (4 B)
-  const size_t per_atom = 16 * 4 + 4 * 7 + 2 + ((flags & PB_MD_VEL_FP64) ? 24 : 16) +
+  // slot (4 B each), x, y, z, type mirrors of rs (16 B), type (2 B),
+  // velocities (16 or 24 B), sysid (4 B)
+  const size_t per_atom = 16 * 4 + 4 * 7 + 16 + 2 + ((flags & PB_MD_VEL_FP64) ? 24 : 16) +
                           (nsys > 1 ? 4 : 0);
   size_t total = 0;
   for (uint32_t s = 0; s < nsys; ++s) {
@@ -410,7 +411,7 @@ int pb_batch_estimate_bytes(const uint32_t *natoms, const float *cells6, const f
     const size_t cols = (size_t)g.n[0] * g.n[1];
     const size_t items = cols * (size_t)(2 + g.n[2] / 4);  // generous: runs per column
     const size_t blocks = blocks_for(natoms[s]);
-    total += per_atom * natoms[s] + 8 * (size_t)g.ncells + 8 * cols +
+    total += per_atom * natoms[s] + 64 + 8 * (size_t)g.ncells + 8 * cols +
              (sizeof(ForceItem) + 32) * items + (sizeof(BlockMap) + 64) * blocks +
              sizeof(SysDesc) + sizeof(SysInt) + sizeof(DevScalars) + sizeof(LJTable) + 64;
   }

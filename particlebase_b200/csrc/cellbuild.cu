@@ -16,7 +16,8 @@
 //   k_scan_*    exclusive scan of per-cell counts -> start[], zero the counts
 //   k_scatter   pid_tmp[start[key] + ticket] = i
 //   k_canon     one warp per cell: order members by (z, particle id), write
-//               pid, slot and the sorted position float4 (type id in .w)
+//               pid, slot, the sorted position float4 (type id in .w) and its
+//               structure-of-arrays mirror (x, y, z, type) for the force kernel
 #include "md.cuh"
 
 namespace pb {
@@ -136,6 +137,18 @@ __global__ void __launch_bounds__(256) k_scatter(CellBufs b) {
   b.pid_tmp[b.start[b.key[i]] + b.within[i]] = i;
 }
 
+// SoA mirror of sorted slot s (atom `me`): the system's sorted atom s - atom0
+// goes to mirror0 + (s - atom0).
+__device__ __forceinline__ void write_mirror(const CellBufs &b, uint32_t me, uint32_t s,
+                                             const float4 &p) {
+  const SysDesc &S = b.sys[system_of(b, me)];
+  const uint32_t m = S.mirror0 + (s - S.atom0);
+  b.xs[m] = p.x;
+  b.ys[m] = p.y;
+  b.zs[m] = p.z;
+  b.ts[m] = (uint32_t)b.type[me];
+}
+
 __device__ __forceinline__ bool canon_before(float za, uint32_t a, float zb, uint32_t b) {
   return za < zb || (za == zb && a < b);
 }
@@ -163,6 +176,7 @@ __global__ void __launch_bounds__(256) k_canon(CellBufs b) {
       b.pid[s] = me;
       b.slot[me] = s;
       b.rs[s] = make_float4(p.x, p.y, p.z, __int_as_float((int)b.type[me]));
+      if (b.xs) write_mirror(b, me, s, p);
     }
   } else {
     // Large cells: O(n^2 / 32) ranking straight from global memory.
@@ -178,6 +192,7 @@ __global__ void __launch_bounds__(256) k_canon(CellBufs b) {
       b.pid[s] = me;
       b.slot[me] = s;
       b.rs[s] = make_float4(p.x, p.y, p.z, __int_as_float((int)b.type[me]));
+      if (b.xs) write_mirror(b, me, s, p);
     }
   }
 }

@@ -110,6 +110,10 @@ void free_cells(Engine &e) {
   dfree(e, e.pid);
   dfree(e, e.slot);
   dfree(e, e.rs);
+  dfree(e, e.xs);
+  dfree(e, e.ys);
+  dfree(e, e.zs);
+  dfree(e, e.ts);
   dfree(e, e.colrank);
   dfree(e, e.colxy);
   dfree(e, e.d_sys);
@@ -353,6 +357,7 @@ int engine_setup_cells(Engine &e) {
   e.item0.assign(e.nsys + 1, 0);
   e.cell0.assign(e.nsys + 1, 0);
   uint64_t ncells = 0;
+  uint32_t mirror = 0;
   e.cap_max = 0;
   for (uint32_t s = 0; s < e.nsys; ++s) {
     SysParams &P = e.sp[s];
@@ -362,7 +367,7 @@ int engine_setup_cells(Engine &e) {
       return fail(e, PB_ERR_ARG, "cell grid needs at least 3 cells per axis (blocknum > 2)");
     P.grid = g;
     const double apc = (double)P.n / g.ncells;
-    P.seg = choose_segment(apc, g.n[2], e.seg_scale);
+    P.seg = choose_segment(apc, g.n[2], e.seg_scale, P.lj_set ? P.lj.nt : 1);
     P.cap = (uint32_t)choose_capacity(apc, P.seg);
     e.cap_max = std::max(e.cap_max, P.cap);
     const std::shared_ptr<const Plan> plan_ref = cached_plan(g, P.seg);
@@ -399,6 +404,8 @@ int engine_setup_cells(Engine &e) {
     D.lj = s;
     D.dt = P.dt;
     D.cap = P.cap;
+    D.mirror0 = mirror;
+    mirror += (P.n + 3u) & ~3u;
     rank_all.insert(rank_all.end(), rank.begin(), rank.end());
     xy_all.insert(xy_all.end(), xy.begin(), xy.end());
     ncells += g.ncells;
@@ -408,13 +415,16 @@ int engine_setup_cells(Engine &e) {
   e.cell0[e.nsys] = (uint32_t)ncells;
   e.ncells = (uint32_t)ncells;
   e.nitems = (uint32_t)items.size();
+  e.mirrorN = mirror + 4u;
   const uint32_t N = e.N, C = e.ncells;
   const uint32_t ntiles = (C + 4095) / 4096;
   bool ok = dalloc(e, &e.key, N) == cudaSuccess && dalloc(e, &e.within, N) == cudaSuccess &&
             dalloc(e, &e.count, C) == cudaSuccess && dalloc(e, &e.start, (size_t)C + 1) == cudaSuccess &&
             dalloc(e, &e.tilesum, ntiles) == cudaSuccess && dalloc(e, &e.pid_tmp, N) == cudaSuccess &&
             dalloc(e, &e.pid, N) == cudaSuccess && dalloc(e, &e.slot, N) == cudaSuccess &&
-            dalloc(e, &e.rs, N) == cudaSuccess && dalloc(e, &e.colrank, rank_all.size()) == cudaSuccess &&
+            dalloc(e, &e.rs, N) == cudaSuccess && dalloc(e, &e.xs, e.mirrorN) == cudaSuccess &&
+            dalloc(e, &e.ys, e.mirrorN) == cudaSuccess && dalloc(e, &e.zs, e.mirrorN) == cudaSuccess &&
+            dalloc(e, &e.ts, e.mirrorN) == cudaSuccess && dalloc(e, &e.colrank, rank_all.size()) == cudaSuccess &&
             dalloc(e, &e.colxy, xy_all.size()) == cudaSuccess &&
             dalloc(e, &e.d_sys, e.nsys) == cudaSuccess && dalloc(e, &e.d_items, items.size()) == cudaSuccess &&
             dalloc(e, &e.d_item0, e.nsys + 1) == cudaSuccess &&
@@ -488,6 +498,10 @@ CellBufs engine_cbufs(Engine &e) {
   b.pid = e.pid;
   b.slot = e.slot;
   b.rs = e.rs;
+  b.xs = e.xs;
+  b.ys = e.ys;
+  b.zs = e.zs;
+  b.ts = e.ts;
   b.status = e.status;
   return b;
 }
@@ -495,6 +509,10 @@ CellBufs engine_cbufs(Engine &e) {
 ForceBufs engine_fbufs(Engine &e) {
   ForceBufs b{};
   b.rs = e.rs;
+  b.xs = e.xs;
+  b.ys = e.ys;
+  b.zs = e.zs;
+  b.ts = e.ts;
   b.start = e.start;
   b.pid = e.pid;
   b.sys = e.d_sys;

@@ -65,6 +65,9 @@ struct Engine {
            *tilesum = nullptr, *pid_tmp = nullptr, *pid = nullptr, *slot = nullptr,
            *colrank = nullptr, *colxy = nullptr, *d_item0 = nullptr;
   float4 *rs = nullptr;
+  float *xs = nullptr, *ys = nullptr, *zs = nullptr;  // SoA mirrors of rs
+  uint32_t *ts = nullptr;
+  uint32_t mirrorN = 0;
   SysDesc *d_sys = nullptr;
   ForceItem *d_items = nullptr;
   uint32_t nitems = 0;

@@ -9,34 +9,43 @@
 // (r_i - r_j) with the minimum image, over the 27-cell stencil.  No 81 N
 // scratch: each atom's force is summed in registers and written once.
 //
-// Work decomposition.  One CTA per work item = (system, x-y column of cells,
-// run of z cells [z0, z1)).  The CTA stages the 3 x 3 neighbour columns over
-// z cells [z0 - 1, z1] (periodic halo cells included) into shared memory with
-// 1-D bulk copies (cp.async.bulk, mbarrier completion, no multicast).
+// Work items.  One work item = (system, x-y column of cells, run of z cells
+// [z0, z1)); its stage is the 3 x 3 neighbour columns over z cells
+// [z0 - 1, z1] (periodic halo cells included).
 //
-// Coordinate frame.  Positions are absolute FP32 coordinates.  Each CTA moves
+// Persistent, warp-specialised CTAs.  Each CTA walks the items blockIdx.x,
+// blockIdx.x + gridDim.x, ... with two stage buffers.  Warp 0 is the
+// producer: for item n + 1 it reads the cell starts, lands the stage in the
+// free buffer with 1-D bulk copies (cp.async.bulk, mbarrier completion, no
+// multicast) from the structure-of-arrays mirrors of the sorted positions,
+// applies the frame shifts, and searches the z window of every (cluster,
+// column).  The other warps are consumers: they compute item n from the other
+// buffer meanwhile, and move on to item n + 1 as soon as the producer
+// publishes it.  mbarriers hand buffers back and forth (full: producer to
+// consumers; empty: consumers to producer); every wait is bounded.
+//
+// Stage layout.  Each staged column is a run of whole 4-atom quads: the bulk
+// copies move 16-byte aligned runs of the x, y, z (and type) mirrors, so up to
+// 3 atoms of the neighbouring cells ride along at each end of a run; the
+// producer turns those into far atoms (x, y = 1e30) whose z keeps the column
+// sorted.  Mirror runs start at the same offset modulo 4 whether a system runs
+// alone or in a batch, so the layout, and every sum, is the same in both.
+//
+// Coordinate frame.  Positions are absolute FP32 coordinates.  Each item moves
 // all staged atoms into one frame by subtracting 0 or L per axis: a neighbour
-// image below the box (atoms near the top face) and, in CTAs on the top face,
+// image below the box (atoms near the top face) and, in items on the top face,
 // every non-wrapped atom, get x - L.  The subtraction only ever applies to
 // coordinates >= L/2, where it is exact (Sterbenz), so displacements x_i - x_j
 // in the frame are the minimum-image displacements with no rounding beyond
 // the subtraction itself, even in a 190-sigma box.  Work items are laid out
 // so that a top-face item's cells all lie above the box middle.
 //
-// Stage layout.  The bulk copies land the 9 staged columns as float4 (x, y,
-// z, type bits) in a landing zone, each column starting at a multiple of 4
-// slots.  One pass applies the frame shift and writes structure-of-arrays
-// planes X, Y, Z (and a type plane) in the same padded slot order; the pad
-// slots of each column hold a far sentinel, so every column is a whole number
-// of 4-atom quads.  The landing zone is then reused for the pair lists.
-//
-// Compute (shared-memory path).  Cells are sorted by z and atoms within a
-// cell by z, so every staged column is one z-sorted array.  A warp takes a
-// cluster of 8 consecutive home atoms (lane & 7) and splits the candidates 4
-// ways (lane >> 3).  Lanes binary-search the z window [z_min - rc, z_max + rc]
-// of the cluster in each of the 9 columns, round it out to whole quads and
-// write the quads of all 9 windows into one per-warp table, so the candidate
-// loop runs over one flat sequence with no per-column tails.  Then
+// Compute.  Cells are sorted by z and atoms within a cell by z, so every
+// staged column is one z-sorted array.  A consumer warp takes a cluster of 8
+// consecutive home atoms (lane & 7) and splits the candidates 4 ways
+// (lane >> 3).  It writes the quads of the cluster's 9 column windows into one
+// flat table (padded to whole chunks with a quad of far atoms), so the
+// candidate loop runs over one sequence with no per-column tails.  Then
 //   phase 1  tests 4 candidates per step (one quad, packed FP32x2 arithmetic)
 //            against rc^2 (1 + 2^-10) and appends the hits to a per-lane index
 //            list in shared memory (no divergent force code);
@@ -45,8 +54,12 @@
 //            r^2 = 0), and evaluates the force, two list entries per step in
 //            packed FP32x2 arithmetic.
 // The 4 partial sums of an atom are combined with two warp shuffles.
-// A CTA whose stage would exceed its shared-memory capacity computes from
-// global memory instead (slower, same result) and raises a status bit.
+// Clusters go to consumers round-robin over the CTA's whole item sequence;
+// a cluster's arithmetic does not depend on which warp runs it, and energy
+// sums are kept per cluster and added in cluster order.  An item whose stage
+// exceeds the shared-memory capacity computes from global memory instead
+// (slower, same result) and raises a status bit.
+#include <algorithm>
 #include <type_traits>
 
 #include "md.cuh"
@@ -55,10 +68,10 @@
 namespace pb {
 namespace {
 
-constexpr int kMaxSeg = 40;     // longest z run of one work item (cells)
-constexpr int kDefaultWarps = 8;
-constexpr int kListLen = 48;    // per-lane pair list entries
+constexpr int kMaxSeg = 32;     // longest z run of one work item (cells)
+constexpr int kListLen = 40;    // per-lane pair list entries
 constexpr int kChunk = 16;      // candidates a lane tests between list checks
+constexpr int kWinCap = 48;     // clusters (or global-path tasks) per item
 constexpr float kFar = 1e30f;   // pad-slot coordinate: never within range
 constexpr float kNoAtom = -1e30f;  // coordinate of a padded home lane
 
@@ -76,39 +89,62 @@ constexpr int kModeLJ = 0;        // truncated LJ (the MD step)
 constexpr int kModeCapped = 1;    // LJ with r^2 floored at (sigma/2)^2 (steepest descent)
 constexpr int kModeSoftCore = 2;  // f0 cos(pi r / 2 rc) along r (initialAnnealing)
 
-struct Stage {
+
+// One work item as the consumers see it (written by the producer).
+template <int NT>
+struct ItemDesc {
   // index within column c of the first staged atom of z cell k (k = 0 is image
   // cell z0 - 1, k = nseg + 1 is image cell z1); entry nseg + 2 is the column's count
   uint32_t off[9][kMaxSeg + 3];
-  uint32_t ps[10];     // first padded slot of each column (multiples of 4); ps[9] = total
+  uint32_t ps[10];     // first slot of each column's region; ps[9] = end
   uint32_t kbase[9];   // packed key of z cell 0 of each column
   float sx[9], sy[9];  // frame shift of each column (0 or L)
   float sz_lo, sz_mid, sz_hi;  // frame shift of staged cell 0, 1..nseg, nseg + 1
-  uint64_t bar;
-  uint32_t total;
-  uint32_t home_g0;    // global sorted index of the first home atom
-  int overflow;
-};
-
-// Padded slots for `cap` staged atoms: each of the 9 columns rounds up to a
-// multiple of 4 (at most 3 pad slots per column), plus one quad of far atoms
-// that pads the last chunk of every quad table.
-__host__ __device__ __forceinline__ uint32_t padded_slots(uint32_t cap) {
-  return ((cap + 27u + 3u) & ~3u) + 4u;
-}
-
-// z windows of a batch of clusters: first quad, quads and flat offset of the
-// window of each (cluster, column), and per cluster the total and the longest.
-constexpr int kWinCap = 64;
-struct Windows {
+  uint32_t item, sys, home_g0, hb, H, nclus, ntask, sentinel, base;
+  int z0, nz, nseg;
+  int skip;            // the system's step budget is spent
+  int overflow;        // the stage exceeds the capacity: global-memory path
+  LJLocal<NT> lj;
+  // z window of each (cluster, column): first quad, quads, flat offset; per
+  // cluster the total and the longest (at least 2)
   uint16_t q0[kWinCap][9], len[kWinCap][9], pre[kWinCap][9];
   uint16_t Q[kWinCap], M[kWinCap];
 };
 
-// Bytes of one warp's pair lists plus its quad table (at most one entry per
-// padded quad of the stage).
+// Producer scratch: global cell starts and counts of the item being staged,
+// and its copy runs (piece p of column c at index 3 c + p).
+struct Scratch {
+  uint32_t gstart[9][kMaxSeg + 3];
+  uint32_t cnt[9][kMaxSeg + 3];
+  uint32_t dst[27], lead[27], n[27], alen[27];
+};
+
+// One stage buffer: X, Y, Z planes and, with more than one type, a type plane.
+struct Planes {
+  float *X, *Y, *Z;
+  uint32_t *T;
+};
+
+// Slots of a stage buffer for `cap` staged atoms: each of up to 3 copy runs
+// per column brings at most 6 neighbouring atoms, plus one quad of far atoms
+// that pads the last chunk of every quad table.
+__host__ __device__ __forceinline__ uint32_t padded_slots(uint32_t cap) {
+  return ((cap + 162u + 3u) & ~3u) + 4u;
+}
+
+__host__ __device__ __forceinline__ uint32_t plane_bytes(uint32_t slots, int nt) {
+  return (slots * (nt > 1 ? 16u : 12u) + 15u) & ~15u;
+}
+
+// Bytes of one consumer warp's pair lists plus its quad table.
 __host__ __device__ __forceinline__ uint32_t warp_bytes(uint32_t slots) {
   return ((32u * kListLen * 2u + (slots / 4u + kChunk) * 2u) + 15u) & ~15u;
+}
+
+// Dynamic shared memory of one CTA: two stage buffers and the consumers' lists.
+__host__ __device__ __forceinline__ uint32_t smem_bytes(uint32_t cap, int consumers, int nt) {
+  const uint32_t slots = padded_slots(cap);
+  return 2u * plane_bytes(slots, nt) + (uint32_t)consumers * warp_bytes(slots);
 }
 
 // Position of flat quad u in a warp's quad table: within each chunk of 16,
@@ -118,14 +154,18 @@ __device__ __forceinline__ uint32_t table_pos(uint32_t u) {
   return (u & ~15u) | ((u & 3u) << 2) | ((u >> 2) & 3u);
 }
 
-// Dynamic shared memory of one CTA: the landing zone (reused for the lists)
-// followed by the X, Y, Z planes and, with more than one type, the type plane.
-__host__ __device__ __forceinline__ uint32_t smem_bytes(uint32_t cap, int warps, int nt) {
-  const uint32_t slots = padded_slots(cap);
-  const uint32_t land = slots * 16u, lists = (uint32_t)warps * warp_bytes(slots);
-  const uint32_t zone = land > lists ? land : lists;
-  const uint32_t planes = (slots * 12u + (nt > 1 ? slots : 0u) + 15u) & ~15u;
-  return zone + planes;
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait that also gives up when the CTA has aborted.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t *bar, uint32_t parity,
+                                                   const volatile int *abort_flag) {
+  for (uint32_t it = 0; it < (1u << 24); ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (*abort_flag) return false;
+  }
+  return false;
 }
 
 // MODE kModeCapped: relaxation force of the steepest-descent path, with the
@@ -217,7 +257,7 @@ __device__ __forceinline__ uint32_t upper_bound_z(const float *Z, uint32_t lo, u
 // candidates phase 1 admitted through its margin and the self pair.
 template <int NT, bool ENERGY, typename Acc, int MODE>
 __device__ __forceinline__ void flush_scalar(const float *X, const float *Y, const float *Z,
-                                             const uint8_t *T, const uint16_t *list,
+                                             const uint32_t *T, const uint16_t *list,
                                              uint32_t cnt, int lane, float xi, float yi, float zi,
                                              int ti, const LJLocal<NT> &lj,
                                              PairAcc<NT, ENERGY, Acc, MODE> &a) {
@@ -235,7 +275,7 @@ __device__ __forceinline__ void flush_scalar(const float *X, const float *Y, con
 // (or past the lane's count) is selected to zero.
 template <int NT, bool ENERGY, int MODE>
 __device__ __forceinline__ void flush_packed(const float *X, const float *Y, const float *Z,
-                                             const uint8_t *T, const uint16_t *list,
+                                             const uint32_t *T, const uint16_t *list,
                                              uint32_t cnt, int lane, float xi, float yi, float zi,
                                              int ti, const LJLocal<NT> &lj,
                                              PairAcc2<ENERGY> &a) {
@@ -297,441 +337,655 @@ __device__ __forceinline__ void flush_packed(const float *X, const float *Y, con
   }
 }
 
-template <int NT, bool ENERGY, typename Acc, int kWarps, int MODE>
-__global__ void __launch_bounds__(kWarps * 32, 24 / kWarps) k_force(ForceBufs b) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ Stage st;
-  __shared__ LJLocal<NT> ljs;
-  __shared__ uint32_t cnt_cell[9][kMaxSeg + 3];
-  __shared__ uint32_t gstart[9][kMaxSeg + 3];
-  __shared__ Windows win;
-  __shared__ double red[4 * 32];
-  // packed phase 2 for FP32 sums of the LJ and capped laws
-  constexpr bool kPacked = std::is_same<Acc, float>::value && MODE != kModeSoftCore;
+// ---- producer ---------------------------------------------------------------
 
-  const uint32_t slots = padded_slots((uint32_t)b.cap);
-  const uint32_t land_bytes = slots * 16u, wbytes = warp_bytes(slots);
-  const uint32_t zone = land_bytes > kWarps * wbytes ? land_bytes : kWarps * wbytes;
-  float4 *land = reinterpret_cast<float4 *>(smem_raw);
-  float *X = reinterpret_cast<float *>(smem_raw + zone);
-  float *Y = X + slots;
-  float *Z = Y + slots;
-  uint8_t *T = reinterpret_cast<uint8_t *>(Z + slots);
+// Barrier of the kProd producer warps only (named barrier 1).
+template <int kProd>
+__device__ __forceinline__ void producer_sync() {
+  asm volatile("bar.sync 1, %0;" ::"r"(kProd * 32) : "memory");
+}
 
-  const ForceItem it = b.items[blockIdx.x];
-  if (b.steps_left != nullptr && b.steps_left[it.sys] == 0) {
-    // a system whose step budget is spent keeps its state; nothing to compute
-    if (ENERGY && threadIdx.x < 4) b.partials[(size_t)blockIdx.x * 4 + threadIdx.x] = 0.0;
-    return;
+// Set up item `item` in descriptor `d` and stage buffer `pl` (the kProd
+// producer warps together).  Returns false when the wait for the bulk copies
+// gave up.
+template <int NT, int MODE, int kProd, int kCons>
+__device__ bool produce_item(const ForceBufs &b, uint32_t item, ItemDesc<NT> &d, Scratch &sc,
+                             const Planes &pl, uint64_t *landed, uint32_t &lphase,
+                             uint32_t &running) {
+  constexpr int kPT = kProd * 32;  // producer threads
+  const int pt = threadIdx.x, lane = pt & 31, pw = pt >> 5;
+  const ForceItem it = b.items[item];
+  const bool skip = b.steps_left != nullptr && b.steps_left[it.sys] == 0;
+  if (pt == 0) {
+    d.item = item;
+    d.sys = it.sys;
+    d.skip = skip;
+    d.overflow = 0;
+    d.H = 0;
+    d.nclus = 0;
+    d.ntask = 0;
+  }
+  if (skip) {  // a system whose step budget is spent keeps its state
+    producer_sync<kProd>();
+    return true;
   }
   const SysDesc &S = b.sys[it.sys];
   const Grid g = S.g;
   const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
   const int z0 = it.z0, z1 = it.z1, nseg = z1 - z0;
   const int ncell = nseg + 2;  // staged cells per column
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-
-  if (threadIdx.x < NT * NT) {
+  for (int t = pt; t < NT * NT; t += kPT) {
     const LJTable &Tb = b.lj[S.lj];
-    const int a = threadIdx.x / NT, c = threadIdx.x % NT;
+    const int a = t / NT, c = t % NT;
     const int k = a * Tb.nt + c;
-    ljs.s2[threadIdx.x] = Tb.s2[k];
-    ljs.e24[threadIdx.x] = Tb.e24[k];
-    ljs.e4[threadIdx.x] = Tb.e4[k];
-    ljs.rc2[threadIdx.x] =
-        MODE == kModeSoftCore ? fminf(Tb.rc2[k], b.sc_rc * b.sc_rc) : Tb.rc2[k];
-    ljs.ush[threadIdx.x] = Tb.ushift[k];
+    d.lj.s2[t] = Tb.s2[k];
+    d.lj.e24[t] = Tb.e24[k];
+    d.lj.e4[t] = Tb.e4[k];
+    d.lj.rc2[t] = MODE == kModeSoftCore ? fminf(Tb.rc2[k], b.sc_rc * b.sc_rc) : Tb.rc2[k];
+    d.lj.ush[t] = Tb.ushift[k];
   }
-  if (threadIdx.x == 0) {
-    ljs.sc_rc = b.sc_rc;
-    ljs.sc_f0 = b.sc_f0;
-  }
-  if (threadIdx.x < 9) {
+  if (pt < 9) {
     const int cx = it.cx, cy = it.cy;
-    const int c = threadIdx.x;
+    const int c = pt;
     const int ax = cx + c / 3 - 1, ay = cy + c % 3 - 1;
     const int wx = ax < 0 ? -1 : (ax >= nx ? 1 : 0);
     const int wy = ay < 0 ? -1 : (ay >= ny ? 1 : 0);
     // frame: F = L on the top face; staged = x + w L - F, so the shift is F - w L
     const float Fx = cx == nx - 1 ? g.L[0] : 0.0f, Fy = cy == ny - 1 ? g.L[1] : 0.0f;
-    st.sx[c] = Fx - (float)wx * g.L[0];
-    st.sy[c] = Fy - (float)wy * g.L[1];
-    st.kbase[c] = it.kbase[c];
+    d.sx[c] = Fx - (float)wx * g.L[0];
+    d.sy[c] = Fy - (float)wy * g.L[1];
+    d.kbase[c] = it.kbase[c];
   }
-  if (threadIdx.x == 0) {
-    const float Fz = z1 == nz ? g.L[2] : 0.0f;
-    st.sz_lo = z0 == 0 ? Fz + g.L[2] : Fz;   // image z0 - 1 wraps below when z0 == 0
-    st.sz_mid = Fz;
-    st.sz_hi = z1 == nz ? Fz - g.L[2] : Fz;  // image z1 wraps above when z1 == nz
+  const float Fz = z1 == nz ? g.L[2] : 0.0f;
+  const float sz_lo = z0 == 0 ? Fz + g.L[2] : Fz;  // image z0 - 1 wraps below when z0 == 0
+  const float sz_hi = z1 == nz ? Fz - g.L[2] : Fz;  // image z1 wraps above when z1 == nz
+  if (pt == 0) {
+    d.sz_lo = sz_lo;
+    d.sz_mid = Fz;
+    d.sz_hi = sz_hi;
+    d.z0 = z0;
+    d.nz = nz;
+    d.nseg = nseg;
+    d.lj.sc_rc = b.sc_rc;
+    d.lj.sc_f0 = b.sc_f0;
   }
-  // counts of the 9 x ncell staged cells, one per thread; cell starts kept
-  for (int t = threadIdx.x; t < 9 * ncell; t += blockDim.x) {
+  // cell starts and counts of the 9 x ncell staged cells
+  for (int t = pt; t < 9 * ncell; t += kPT) {
     const int c = t / ncell, k = t % ncell;
     const int zc = (z0 - 1 + k + nz) % nz;
     const uint32_t key = it.kbase[c] + (uint32_t)zc;
     const uint32_t s0 = b.start[key];
-    gstart[c][k] = s0;
-    cnt_cell[c][k] = b.start[key + 1] - s0;
+    sc.gstart[c][k] = s0;
+    sc.cnt[c][k] = b.start[key + 1] - s0;
   }
-  __syncthreads();
+  producer_sync<kProd>();
   // exclusive prefix over the cells of each column, one warp per column
-  for (int c = warp; c < 9; c += kWarps) {
+  for (int c = pw; c < 9; c += kProd) {
     uint32_t run = 0;
     for (int base = 0; base < ncell; base += 32) {
       const int k = base + lane;
-      const uint32_t v = k < ncell ? cnt_cell[c][k] : 0u;
+      const uint32_t v = k < ncell ? sc.cnt[c][k] : 0u;
       uint32_t incl = v;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
       }
-      if (k < ncell) st.off[c][k] = run + incl - v;
+      if (k < ncell) d.off[c][k] = run + incl - v;
       run += __shfl_sync(0xffffffffu, incl, 31);
     }
-    if (lane == 0) st.off[c][ncell] = run;
+    if (lane == 0) d.off[c][ncell] = run;
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t p = 0, run = 0;
-    for (int c = 0; c < 9; ++c) {
-      const uint32_t n = st.off[c][ncell];
-      st.ps[c] = p;
-      p += (n + 3u) & ~3u;
-      run += n;
+  producer_sync<kProd>();
+  // copy runs: piece 0 = image cell z0 - 1 when z0 == 0, piece 2 = image cell
+  // z1 when z1 == nz, piece 1 = the cells between (consecutive z, one run)
+  const int a_end = z0 == 0 ? 1 : 0, c_beg = z1 == nz ? ncell - 1 : ncell;
+  const uint32_t H = d.off[4][nseg + 1] - d.off[4][1];
+  const uint32_t nclus = (H + 7) / 8;
+  if (pw == 0) {
+    uint32_t n = 0, m0 = 0, ma = 0, alen = 0;
+    if (lane < 27) {
+      const int c = lane / 3, p = lane % 3;
+      const int k0 = p == 0 ? 0 : (p == 1 ? a_end : c_beg);
+      const int k1 = p == 0 ? a_end : (p == 1 ? c_beg : ncell);
+      n = d.off[c][k1] - d.off[c][k0];
+      if (n > 0) {
+        m0 = S.mirror0 + (sc.gstart[c][k0] - S.atom0);
+        ma = m0 & ~3u;
+        alen = ((m0 + n + 3u) & ~3u) - ma;
+      }
     }
-    st.ps[9] = p;
-    st.total = run;
+    uint32_t incl = alen;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const uint32_t dst = incl - alen;
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    if (lane < 27) {
+      sc.dst[lane] = dst;
+      sc.lead[lane] = m0 - ma;
+      sc.n[lane] = n;
+      sc.alen[lane] = alen;
+      if (lane % 3 == 0) d.ps[lane / 3] = dst;
+    }
     // the system's own capacity decides: the same path alone or batched
-    // (4 slots stay free for the sentinel quad)
-    st.overflow = p + 4u > padded_slots(S.cap);
-    st.home_g0 = gstart[4][1];
-    if (!st.overflow && run > 0) {
-      mbar_init(&st.bar, 9);
-      mbar_fence_init();
+    const bool overflow = total + 4u > padded_slots(S.cap) || nclus > (uint32_t)kWinCap;
+    if (lane == 0) {
+      d.ps[9] = total;
+      d.H = H;
+      d.home_g0 = sc.gstart[4][1];
+      d.overflow = overflow;
+      if (overflow) {
+        d.ntask = min((H + 31) / 32, (uint32_t)kWinCap);
+        atomicOr(&b.status[it.sys], kStatusSmemOverflow);
+      }
+    }
+    if (!overflow && total > 0) {
+      uint32_t bytes = alen * 4u * (NT > 1 ? 4u : 3u);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+      if (lane == 0) mbar_arrive_expect_tx(landed, bytes);
+      __syncwarp();
+      if (lane < 27 && alen > 0) {
+        bulk_g2s(pl.X + dst, b.xs + ma, alen * 4u, landed);
+        bulk_g2s(pl.Y + dst, b.ys + ma, alen * 4u, landed);
+        bulk_g2s(pl.Z + dst, b.zs + ma, alen * 4u, landed);
+        if (NT > 1) bulk_g2s(pl.T + dst, b.ts + ma, alen * 4u, landed);
+      }
     }
   }
-  __syncthreads();
-  const bool overflow = st.overflow;
-  if (!overflow && st.total > 0) {
-    if (threadIdx.x < 9) {
-      // column c: up to three contiguous runs (below halo, main, above halo)
-      const int c = threadIdx.x;
-      const uint32_t base = st.ps[c];
-      mbar_arrive_expect_tx(&st.bar, st.off[c][ncell] * 16u);
-      int k = 0;
-      while (k < ncell) {
-        const int zc = (z0 - 1 + k + nz) % nz;
-        int kend = k;
-        while (kend + 1 < ncell && ((z0 - 1 + kend + 1 + nz) % nz) == zc + (kend + 1 - k)) ++kend;
-        const uint32_t g0 = gstart[c][k];
-        const uint32_t g1 = gstart[c][kend] + cnt_cell[c][kend];
-        if (g1 > g0) bulk_g2s(&land[base + st.off[c][k]], &b.rs[g0], (g1 - g0) * 16u, &st.bar);
-        k = kend + 1;
+  producer_sync<kProd>();
+  if (d.overflow) return true;
+  const uint32_t total = d.ps[9];
+  if (total > 0) {
+    bool ok = pt != 0 || mbar_wait_bounded(landed, lphase);
+    lphase ^= 1u;
+    // all producer threads learn the outcome through the barrier
+    if (pt == 0 && !ok) {
+      atomicOr(&b.status[it.sys], kStatusWaitTimeout);
+      // give the copies in flight a second bounded wait before giving up
+      mbar_wait_bounded(landed, lphase ^ 1u);
+      d.skip = 2;
+    }
+    producer_sync<kProd>();
+    if (d.skip == 2) return false;
+    // frame shifts of the real atoms of each run
+    for (int p = 0; p < 27; ++p) {
+      const int c = p / 3, pp = p % 3;
+      const float sx = d.sx[c], sy = d.sy[c];
+      const float sz = pp == 0 ? sz_lo : (pp == 1 ? Fz : sz_hi);
+      if (sx == 0.f && sy == 0.f && sz == 0.f) continue;
+      const uint32_t s0 = sc.dst[p] + sc.lead[p], s1 = s0 + sc.n[p];
+      for (uint32_t s = s0 + pt; s < s1; s += kPT) {
+        pl.X[s] -= sx;
+        pl.Y[s] -= sy;
+        pl.Z[s] -= sz;
       }
     }
-    // one thread polls the barrier; the others sleep at the CTA barrier and
-    // see the copied data through it
-    const bool ok = threadIdx.x != 0 || mbar_wait_bounded(&st.bar, 0);
-    if (__syncthreads_or(!ok)) {
-      // give the copies in flight a second bounded wait before the CTA leaves
-      if (threadIdx.x == 0) {
-        atomicOr(&b.status[it.sys], kStatusWaitTimeout);
-        mbar_wait_bounded(&st.bar, 0);
+    producer_sync<kProd>();
+    // neighbouring atoms that rode along become far atoms that keep z sorted
+    if (pt < 27 && sc.alen[pt] > 0) {
+      const uint32_t dst = sc.dst[pt], s0 = dst + sc.lead[pt], s1 = s0 + sc.n[pt];
+      const float zlo = pl.Z[s0], zhi = pl.Z[s1 - 1];
+      for (uint32_t s = dst; s < s0; ++s) {
+        pl.X[s] = kFar;
+        pl.Y[s] = kFar;
+        pl.Z[s] = zlo;
+        if (NT > 1) pl.T[s] = 0u;
       }
-      return;
+      for (uint32_t s = s1; s < dst + sc.alen[pt]; ++s) {
+        pl.X[s] = kFar;
+        pl.Y[s] = kFar;
+        pl.Z[s] = zhi;
+        if (NT > 1) pl.T[s] = 0u;
+      }
     }
-    // frame shift and SoA planes; pad slots get the far sentinel
+  }
+  if (pt >= 32 * (kProd - 1) && pt < 32 * (kProd - 1) + 4) {
+    // the quad of far atoms that pads the last chunk of a table
+    const uint32_t s = total + (uint32_t)(pt - 32 * (kProd - 1));
+    pl.X[s] = kFar;
+    pl.Y[s] = kFar;
+    pl.Z[s] = kFar;
+    if (NT > 1) pl.T[s] = 0u;
+  }
+  producer_sync<kProd>();
+  // z windows of every (cluster, column)
+  const int hp = 4 * 3 + 1;  // the home column's middle run holds home cells 1..nseg
+  const uint32_t hb = sc.dst[hp] + sc.lead[hp] + (d.off[4][1] - d.off[4][a_end]);
+  float rcmax2 = 0.f;
+  for (int k = 0; k < NT * NT; ++k) rcmax2 = fmaxf(rcmax2, d.lj.rc2[k]);
+  const float rcw = sqrtf(rcmax2) * 1.00001f + 1e-5f;
+  for (uint32_t t = pt; t < 9u * nclus; t += kPT) {
+    const uint32_t k = t / 9u, c = t - 9u * k;
+    const float zmin = pl.Z[hb + k * 8];
+    const float zmax = pl.Z[hb + min(k * 8 + 7, H - 1)];
+    const uint32_t lo = d.ps[c], hi = d.ps[c + 1];
+    const uint32_t a = lower_bound_z(pl.Z, lo, hi, zmin - rcw) >> 2;
+    const uint32_t e = (upper_bound_z(pl.Z, lo, hi, zmax + rcw) + 3u) >> 2;
+    d.q0[k][c] = (uint16_t)a;
+    // empty unless ordered (an unsorted column, e.g. NaN positions, can
+    // invert the two searches)
+    d.len[k][c] = (uint16_t)(e > a ? e - a : 0u);
+  }
+  producer_sync<kProd>();
+  for (uint32_t k = pt; k < nclus; k += kPT) {
+    uint32_t s = 0, m = 2;
     for (int c = 0; c < 9; ++c) {
-      const uint32_t p0 = st.ps[c], p1 = st.ps[c + 1];
-      const uint32_t n = st.off[c][ncell];
-      const uint32_t lo_end = st.off[c][1];
-      const uint32_t hi_beg = st.off[c][nseg + 1];
-      const float sx = st.sx[c], sy = st.sy[c];
-      for (uint32_t s = p0 + threadIdx.x; s < p1; s += blockDim.x) {
-        const uint32_t r = s - p0;
-        float x = kFar, y = kFar, z = kFar;
-        uint8_t ty = 0;
-        if (r < n) {
-          const float4 p = land[s];
-          const float sz = r < lo_end ? st.sz_lo : (r < hi_beg ? st.sz_mid : st.sz_hi);
-          x = p.x - sx;
-          y = p.y - sy;
-          z = p.z - sz;
-          ty = (uint8_t)__float_as_int(p.w);
-        }
-        X[s] = x;
-        Y[s] = y;
-        Z[s] = z;
-        if (NT > 1) T[s] = ty;
-      }
+      d.pre[k][c] = (uint16_t)s;
+      s += d.len[k][c];
+      m = max(m, (uint32_t)d.len[k][c]);
     }
-    if (threadIdx.x < 4) {  // the sentinel quad that pads the last chunk of a table
-      const uint32_t s = st.ps[9] + threadIdx.x;
-      X[s] = kFar;
-      Y[s] = kFar;
-      Z[s] = kFar;
-      if (NT > 1) T[s] = 0;
-    }
-    __syncthreads();  // the landing zone is free from here on
-  } else if (overflow && threadIdx.x == 0) {
-    atomicOr(&b.status[it.sys], kStatusSmemOverflow);
+    d.Q[k] = (uint16_t)s;
+    d.M[k] = (uint16_t)m;
   }
+  if (pt == 0) {
+    d.hb = hb;
+    d.nclus = nclus;
+    d.sentinel = total / 4u;
+    d.base = running % (uint32_t)kCons;
+  }
+  running += nclus;
+  producer_sync<kProd>();
+  return true;
+}
 
-  Acc pe = 0, pes = 0, vir = 0;
-  uint32_t npairs = 0;
-
-  if (!overflow && st.total > 0) {
-    const uint32_t H = st.off[4][nseg + 1] - st.off[4][1];
-    const uint32_t hb = st.ps[4] + st.off[4][1];  // slot of home atom 0
-    const uint32_t sentinel = st.ps[9] / 4u;       // quad of far atoms
-    uint16_t *mylist = reinterpret_cast<uint16_t *>(smem_raw + (size_t)warp * wbytes);
-    uint16_t *tb = mylist + 32 * kListLen;
-    const int il = lane & 7, q = lane >> 3;
-    float rcmax2 = 0.f;
-    for (int k = 0; k < NT * NT; ++k) rcmax2 = fmaxf(rcmax2, ljs.rc2[k]);
-    const float rcw = sqrtf(rcmax2) * 1.00001f + 1e-5f;
-    // phase-1 bound with a margin: a superset of the exact test of phase 2
-    const float2 nrc = make_float2(-rcmax2 * (1.0f + 1.0f / 1024.0f),
-                                   -rcmax2 * (1.0f + 1.0f / 1024.0f));
-    const float2 m1 = make_float2(-1.0f, -1.0f);
-    const float4 *X4 = reinterpret_cast<const float4 *>(X);
-    const float4 *Y4 = reinterpret_cast<const float4 *>(Y);
-    const float4 *Z4 = reinterpret_cast<const float4 *>(Z);
-    const uint32_t nclus = (H + 7) / 8;
-    for (uint32_t cb = 0; cb < nclus; cb += kWinCap) {
-      const uint32_t nb = min((uint32_t)kWinCap, nclus - cb);
-      // z windows of every (cluster, column) of this batch, one per thread
-      for (uint32_t t = threadIdx.x; t < 9u * nb; t += blockDim.x) {
-        const uint32_t k = t / 9u, c = t - 9u * k;
-        const uint32_t cl = cb + k;
-        const float zmin = Z[hb + cl * 8];
-        const float zmax = Z[hb + min(cl * 8 + 7, H - 1)];
-        const uint32_t lo = st.ps[c], hi = lo + st.off[c][ncell];
-        const uint32_t a = lower_bound_z(Z, lo, hi, zmin - rcw) >> 2;
-        const uint32_t e = (upper_bound_z(Z, lo, hi, zmax + rcw) + 3u) >> 2;
-        win.q0[k][c] = (uint16_t)a;
-        // empty unless ordered (an unsorted column, e.g. NaN positions, can
-        // invert the two searches)
-        win.len[k][c] = (uint16_t)(e > a ? e - a : 0u);
-      }
-      __syncthreads();
-      for (uint32_t k = threadIdx.x; k < nb; k += blockDim.x) {
-        uint32_t s = 0, m = 2;
-        for (int c = 0; c < 9; ++c) {
-          win.pre[k][c] = (uint16_t)s;
-          s += win.len[k][c];
-          m = max(m, (uint32_t)win.len[k][c]);
-        }
-        win.Q[k] = (uint16_t)s;
-        win.M[k] = (uint16_t)m;
-      }
-      __syncthreads();
-      for (uint32_t k = warp; k < nb; k += kWarps) {
-        const uint32_t cl = cb + k;
-        const uint32_t h = cl * 8 + il;
-        const bool valid = h < H;
-        const uint32_t hs = hb + (valid ? h : H - 1);
-        const float xi = valid ? X[hs] : kNoAtom;
-        const float yi = valid ? Y[hs] : kNoAtom;
-        const float zi = valid ? Z[hs] : kNoAtom;
-        const int ti = NT == 1 ? 0 : (int)T[hs];
-        // the warp's quad table: lanes cover (column, index) pairs, column =
-        // idx / M by a multiply-high (exact while 9 M^2 < 2^32)
-        const uint32_t Q = win.Q[k], M = win.M[k];
-        const uint32_t magic = 0xffffffffu / M + 1u;
-        for (uint32_t idx = lane; idx < 9u * M; idx += 32) {
-          const uint32_t c = __umulhi(idx, magic), i = idx - c * M;
-          if (i < win.len[k][c]) tb[table_pos(win.pre[k][c] + i)] = (uint16_t)(win.q0[k][c] + i);
-        }
-        for (uint32_t u = Q + lane; u < ((Q + 15u) & ~15u); u += 32)
-          tb[table_pos(u)] = (uint16_t)sentinel;
-        __syncwarp();
-
-        PairAcc<NT, ENERGY, Acc, MODE> acc;
-        PairAcc2<ENERGY> acc2;
-        auto flush = [&](uint32_t cnt) {
-          if constexpr (kPacked) {
-            flush_packed<NT, ENERGY, MODE>(X, Y, Z, T, mylist, cnt, lane, xi, yi, zi, ti, ljs,
-                                           acc2);
-          } else {
-            flush_scalar<NT, ENERGY, Acc, MODE>(X, Y, Z, T, mylist, cnt, lane, xi, yi, zi, ti,
-                                                ljs, acc);
-          }
-        };
-        const float2 xi2 = make_float2(xi, xi), yi2 = make_float2(yi, yi), zi2 = make_float2(zi, zi);
-        uint16_t *out = mylist + lane;
-        // lane q tests quads u = q, q + 4, ... of the flat sequence, 4 per
-        // chunk; the table pads the last chunk with the sentinel quad
-        for (uint32_t u0 = 0; u0 < Q; u0 += kChunk) {
-          const uint32_t cnt = (uint32_t)(out - (mylist + lane)) >> 5;
-          if (__reduce_max_sync(0xffffffffu, cnt) > (uint32_t)(kListLen - kChunk)) {
-            flush(cnt);
-            __syncwarp();
-            out = mylist + lane;
-          }
-          const uint2 qq = *reinterpret_cast<const uint2 *>(tb + u0 + 4 * q);
-          const uint32_t quads[4] = {qq.x & 0xffffu, qq.x >> 16, qq.y & 0xffffu, qq.y >> 16};
-#pragma unroll
-          for (int kk = 0; kk < kChunk / 4; ++kk) {
-            const uint32_t quad = quads[kk];
-            const float4 x4 = X4[quad], y4 = Y4[quad], z4 = Z4[quad];
-            const float2 dxa = __ffma2_rn(make_float2(x4.x, x4.y), m1, xi2);
-            const float2 dxb = __ffma2_rn(make_float2(x4.z, x4.w), m1, xi2);
-            const float2 dya = __ffma2_rn(make_float2(y4.x, y4.y), m1, yi2);
-            const float2 dyb = __ffma2_rn(make_float2(y4.z, y4.w), m1, yi2);
-            const float2 dza = __ffma2_rn(make_float2(z4.x, z4.y), m1, zi2);
-            const float2 dzb = __ffma2_rn(make_float2(z4.z, z4.w), m1, zi2);
-            const float2 da =
-                __ffma2_rn(dza, dza, __ffma2_rn(dya, dya, __ffma2_rn(dxa, dxa, nrc)));
-            const float2 db =
-                __ffma2_rn(dzb, dzb, __ffma2_rn(dyb, dyb, __ffma2_rn(dxb, dxb, nrc)));
-            // the stores are in bounds whether or not they are kept: the check
-            // above leaves room for every candidate of this chunk
-            const uint32_t s = quad * 4u;
-            out[0] = (uint16_t)s;
-            out += da.x < 0.0f ? 32 : 0;
-            out[0] = (uint16_t)(s + 1u);
-            out += da.y < 0.0f ? 32 : 0;
-            out[0] = (uint16_t)(s + 2u);
-            out += db.x < 0.0f ? 32 : 0;
-            out[0] = (uint16_t)(s + 3u);
-            out += db.y < 0.0f ? 32 : 0;
-          }
-        }
-        flush((uint32_t)(out - (mylist + lane)) >> 5);
-        __syncwarp();
-        float fx, fy, fz;
-        if constexpr (kPacked) {
-          fx = acc2.fx.x + acc2.fx.y;
-          fy = acc2.fy.x + acc2.fy.y;
-          fz = acc2.fz.x + acc2.fz.y;
-#pragma unroll
-          for (int o = 8; o < 32; o <<= 1) {
-            fx += __shfl_xor_sync(0xffffffffu, fx, o);
-            fy += __shfl_xor_sync(0xffffffffu, fy, o);
-            fz += __shfl_xor_sync(0xffffffffu, fz, o);
-          }
-          if (ENERGY) {
-            pe += (Acc)(acc2.pe.x + acc2.pe.y);
-            pes += (Acc)(acc2.pes.x + acc2.pes.y);
-            vir += (Acc)(acc2.vir.x + acc2.vir.y);
-            npairs += acc2.n;
-          }
-        } else {
-          // combine the 4 partial sums of each home atom (lanes il, il+8, il+16, il+24)
-#pragma unroll
-          for (int o = 8; o < 32; o <<= 1) {
-            acc.fx += __shfl_xor_sync(0xffffffffu, acc.fx, o);
-            acc.fy += __shfl_xor_sync(0xffffffffu, acc.fy, o);
-            acc.fz += __shfl_xor_sync(0xffffffffu, acc.fz, o);
-          }
-          fx = (float)acc.fx;
-          fy = (float)acc.fy;
-          fz = (float)acc.fz;
-          if (ENERGY) {
-            pe += acc.pe;
-            pes += acc.pes;
-            vir += acc.vir;
-            npairs += acc.n;
-          }
-        }
-        if (valid && q == 0) {
-          const uint32_t gh = st.home_g0 + h;
-          b.F[b.pid[gh]] = make_float4(fx, fy, fz, 0.0f);
-        }
-      }
-      __syncthreads();  // the next batch reuses the window arrays
+// Energy partials of a finished item: its per-cluster (or per-task) sums in
+// cluster order.
+template <int NT>
+__device__ void write_partials(const ForceBufs &b, const ItemDesc<NT> &d, const double (*e)[4]) {
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  if (!d.skip) {
+    const uint32_t n = d.overflow ? d.ntask : d.nclus;
+    for (uint32_t k = 0; k < n; ++k) {
+      v[0] += e[k][0];
+      v[1] += e[k][1];
+      v[2] += e[k][2];
+      v[3] += e[k][3];
     }
-  } else if (overflow) {
-    // Global-memory path: 32 consecutive home atoms per warp, one per lane.
-    const uint32_t hbeg = st.off[4][1];
-    const uint32_t H = st.off[4][nseg + 1] - hbeg;
-    for (uint32_t t = warp; t * 32 < H; t += kWarps) {
-      const uint32_t h = t * 32 + lane;
-      const bool valid = h < H;
-      const uint32_t hh = valid ? h : H - 1;
-      // home cell (staged index k in [1, nseg]) of this lane, and the warp's span
-      int lo = 1, hi = nseg;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (st.off[4][mid] - hbeg <= hh) lo = mid; else hi = mid - 1;
-      }
-      const int kmin = __reduce_min_sync(0xffffffffu, lo);
-      const int kmax = __reduce_max_sync(0xffffffffu, lo);
-      const uint32_t gh = st.home_g0 + hh;
-      const float4 p = b.rs[gh];
-      const float xi = p.x - st.sx[4], yi = p.y - st.sy[4], zi = p.z - st.sz_mid;
-      const int ti = NT == 1 ? 0 : __float_as_int(p.w);
-      PairAcc<NT, ENERGY, Acc, MODE> acc;
-      for (int c = 0; c < 9; ++c) {
-        for (int k = kmin - 1; k <= kmax + 1; ++k) {
-          const int zc = (z0 - 1 + k + nz) % nz;
-          const uint32_t key = st.kbase[c] + (uint32_t)zc;
-          const float sz = k == 0 ? st.sz_lo : (k == nseg + 1 ? st.sz_hi : st.sz_mid);
-          if (c == 4)
-            global_range<NT, ENERGY, true, Acc, MODE>(b.rs, b.start[key], b.start[key + 1], xi, yi,
-                                                      zi, ti, st.sx[c], st.sy[c], sz, gh, ljs, acc);
-          else
-            global_range<NT, ENERGY, false, Acc, MODE>(b.rs, b.start[key], b.start[key + 1], xi,
-                                                       yi, zi, ti, st.sx[c], st.sy[c], sz, 0, ljs,
-                                                       acc);
-        }
-      }
-      if (valid) {
-        b.F[b.pid[gh]] = make_float4((float)acc.fx, (float)acc.fy, (float)acc.fz, 0.0f);
-        if (ENERGY) {
-          pe += acc.pe;
-          pes += acc.pes;
-          vir += acc.vir;
-          npairs += acc.n;
-        }
-      }
+  }
+  for (int k = 0; k < 4; ++k) b.partials[(size_t)d.item * 4 + k] = v[k];
+}
+
+// ---- consumers --------------------------------------------------------------
+
+// One cluster of 8 home atoms (consumer warp, all 32 lanes); returns the
+// cluster's energy sums in lane 0 (pe, shifted pe, virial, pairs).
+template <int NT, bool ENERGY, typename Acc, int MODE>
+__device__ __forceinline__ void consume_cluster(const ForceBufs &b, const ItemDesc<NT> &d,
+                                                const Planes &pl, uint32_t cl, uint16_t *mylist,
+                                                uint16_t *tb, double (&ce)[4]) {
+  constexpr bool kPacked = std::is_same<Acc, float>::value && MODE != kModeSoftCore;
+  const int lane = threadIdx.x & 31;
+  const int il = lane & 7, q = lane >> 3;
+  const float *X = pl.X, *Y = pl.Y, *Z = pl.Z;
+  const uint32_t *T = pl.T;
+  const uint32_t H = d.H, hb = d.hb;
+  const uint32_t h = cl * 8 + il;
+  const bool valid = h < H;
+  const uint32_t hs = hb + (valid ? h : H - 1);
+  const float xi = valid ? X[hs] : kNoAtom;
+  const float yi = valid ? Y[hs] : kNoAtom;
+  const float zi = valid ? Z[hs] : kNoAtom;
+  const int ti = NT == 1 ? 0 : (int)T[hs];
+  // the warp's quad table: lanes cover (column, index) pairs, column = idx / M
+  // by a multiply-high (exact while 9 M^2 < 2^32)
+  const uint32_t Q = d.Q[cl], M = d.M[cl];
+  const uint32_t magic = 0xffffffffu / M + 1u;
+  for (uint32_t idx = lane; idx < 9u * M; idx += 32) {
+    const uint32_t c = __umulhi(idx, magic), i = idx - c * M;
+    if (i < d.len[cl][c]) tb[table_pos(d.pre[cl][c] + i)] = (uint16_t)(d.q0[cl][c] + i);
+  }
+  for (uint32_t u = Q + lane; u < ((Q + 15u) & ~15u); u += 32)
+    tb[table_pos(u)] = (uint16_t)d.sentinel;
+  __syncwarp();
+
+  float rcmax2 = 0.f;
+  for (int k = 0; k < NT * NT; ++k) rcmax2 = fmaxf(rcmax2, d.lj.rc2[k]);
+  // phase-1 bound with a margin: a superset of the exact test of phase 2
+  const float2 nrc = make_float2(-rcmax2 * (1.0f + 1.0f / 1024.0f),
+                                 -rcmax2 * (1.0f + 1.0f / 1024.0f));
+  const float2 m1 = make_float2(-1.0f, -1.0f);
+  const float4 *X4 = reinterpret_cast<const float4 *>(X);
+  const float4 *Y4 = reinterpret_cast<const float4 *>(Y);
+  const float4 *Z4 = reinterpret_cast<const float4 *>(Z);
+  PairAcc<NT, ENERGY, Acc, MODE> acc;
+  PairAcc2<ENERGY> acc2;
+  auto flush = [&](uint32_t cnt) {
+    if constexpr (kPacked) {
+      flush_packed<NT, ENERGY, MODE>(X, Y, Z, T, mylist, cnt, lane, xi, yi, zi, ti, d.lj, acc2);
+    } else {
+      flush_scalar<NT, ENERGY, Acc, MODE>(X, Y, Z, T, mylist, cnt, lane, xi, yi, zi, ti, d.lj,
+                                          acc);
     }
+  };
+  const float2 xi2 = make_float2(xi, xi), yi2 = make_float2(yi, yi), zi2 = make_float2(zi, zi);
+  uint16_t *out = mylist + lane;
+  // lane q tests quads u = q, q + 4, ... of the flat sequence, 4 per chunk; the
+  // table pads the last chunk with the quad of far atoms
+  for (uint32_t u0 = 0; u0 < Q; u0 += kChunk) {
+    const uint32_t cnt = (uint32_t)(out - (mylist + lane)) >> 5;
+    if (__reduce_max_sync(0xffffffffu, cnt) > (uint32_t)(kListLen - kChunk)) {
+      flush(cnt);
+      __syncwarp();
+      out = mylist + lane;
+    }
+    const uint2 qq = *reinterpret_cast<const uint2 *>(tb + u0 + 4 * q);
+    const uint32_t quads[4] = {qq.x & 0xffffu, qq.x >> 16, qq.y & 0xffffu, qq.y >> 16};
+#pragma unroll
+    for (int kk = 0; kk < kChunk / 4; ++kk) {
+      const uint32_t quad = quads[kk];
+      const float4 x4 = X4[quad], y4 = Y4[quad], z4 = Z4[quad];
+      const float2 dxa = __ffma2_rn(make_float2(x4.x, x4.y), m1, xi2);
+      const float2 dxb = __ffma2_rn(make_float2(x4.z, x4.w), m1, xi2);
+      const float2 dya = __ffma2_rn(make_float2(y4.x, y4.y), m1, yi2);
+      const float2 dyb = __ffma2_rn(make_float2(y4.z, y4.w), m1, yi2);
+      const float2 dza = __ffma2_rn(make_float2(z4.x, z4.y), m1, zi2);
+      const float2 dzb = __ffma2_rn(make_float2(z4.z, z4.w), m1, zi2);
+      const float2 da = __ffma2_rn(dza, dza, __ffma2_rn(dya, dya, __ffma2_rn(dxa, dxa, nrc)));
+      const float2 db = __ffma2_rn(dzb, dzb, __ffma2_rn(dyb, dyb, __ffma2_rn(dxb, dxb, nrc)));
+      // the stores are in bounds whether or not they are kept: the check above
+      // leaves room for every candidate of this chunk
+      const uint32_t s = quad * 4u;
+      out[0] = (uint16_t)s;
+      out += da.x < 0.0f ? 32 : 0;
+      out[0] = (uint16_t)(s + 1u);
+      out += da.y < 0.0f ? 32 : 0;
+      out[0] = (uint16_t)(s + 2u);
+      out += db.x < 0.0f ? 32 : 0;
+      out[0] = (uint16_t)(s + 3u);
+      out += db.y < 0.0f ? 32 : 0;
+    }
+  }
+  flush((uint32_t)(out - (mylist + lane)) >> 5);
+  __syncwarp();
+  float fx, fy, fz;
+  Acc e0 = 0, e1 = 0, e2 = 0;
+  uint32_t e3 = 0;
+  if constexpr (kPacked) {
+    fx = acc2.fx.x + acc2.fx.y;
+    fy = acc2.fy.x + acc2.fy.y;
+    fz = acc2.fz.x + acc2.fz.y;
+#pragma unroll
+    for (int o = 8; o < 32; o <<= 1) {
+      fx += __shfl_xor_sync(0xffffffffu, fx, o);
+      fy += __shfl_xor_sync(0xffffffffu, fy, o);
+      fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    }
+    if (ENERGY) {
+      e0 = acc2.pe.x + acc2.pe.y;
+      e1 = acc2.pes.x + acc2.pes.y;
+      e2 = acc2.vir.x + acc2.vir.y;
+      e3 = acc2.n;
+    }
+  } else {
+    // combine the 4 partial sums of each home atom (lanes il, il+8, il+16, il+24)
+#pragma unroll
+    for (int o = 8; o < 32; o <<= 1) {
+      acc.fx += __shfl_xor_sync(0xffffffffu, acc.fx, o);
+      acc.fy += __shfl_xor_sync(0xffffffffu, acc.fy, o);
+      acc.fz += __shfl_xor_sync(0xffffffffu, acc.fz, o);
+    }
+    fx = (float)acc.fx;
+    fy = (float)acc.fy;
+    fz = (float)acc.fz;
+    if (ENERGY) {
+      e0 = acc.pe;
+      e1 = acc.pes;
+      e2 = acc.vir;
+      e3 = acc.n;
+    }
+  }
+  if (valid && q == 0) {
+    const uint32_t gh = d.home_g0 + h;
+    b.F[b.pid[gh]] = make_float4(fx, fy, fz, 0.0f);
   }
   if (ENERGY) {
-    double v[4] = {(double)pe, (double)pes, (double)vir, (double)npairs};
-    block_sum<4>(v, red);
-    if (threadIdx.x == 0) {
-      b.partials[(size_t)blockIdx.x * 4 + 0] = v[0];
-      b.partials[(size_t)blockIdx.x * 4 + 1] = v[1];
-      b.partials[(size_t)blockIdx.x * 4 + 2] = v[2];
-      b.partials[(size_t)blockIdx.x * 4 + 3] = v[3];
-    }
+    ce[0] = warp_sum((double)e0);
+    ce[1] = warp_sum((double)e1);
+    ce[2] = warp_sum((double)e2);
+    ce[3] = (double)warp_sum(e3);
   }
 }
 
-template <int NT, bool E, typename Acc, int W, int MODE = kModeLJ>
+// Global-memory path of an item whose stage does not fit: task t covers the
+// groups of 32 consecutive home atoms t, t + ntask, ...; lanes are atoms.
+template <int NT, bool ENERGY, typename Acc, int MODE>
+__device__ void consume_task_global(const ForceBufs &b, const ItemDesc<NT> &d, uint32_t t,
+                                    double (&ce)[4]) {
+  const int lane = threadIdx.x & 31;
+  const int nseg = d.nseg, z0 = d.z0, nz = d.nz;
+  const uint32_t hbeg = d.off[4][1];
+  const uint32_t H = d.H;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (uint32_t gi = t; gi * 32 < H; gi += d.ntask) {
+    const uint32_t h = gi * 32 + lane;
+    const bool valid = h < H;
+    const uint32_t hh = valid ? h : H - 1;
+    // home cell (staged index k in [1, nseg]) of this lane, and the warp's span
+    int lo = 1, hi = nseg;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (d.off[4][mid] - hbeg <= hh) lo = mid; else hi = mid - 1;
+    }
+    const int kmin = __reduce_min_sync(0xffffffffu, lo);
+    const int kmax = __reduce_max_sync(0xffffffffu, lo);
+    const uint32_t gh = d.home_g0 + hh;
+    const float4 p = b.rs[gh];
+    const float xi = p.x - d.sx[4], yi = p.y - d.sy[4], zi = p.z - d.sz_mid;
+    const int ti = NT == 1 ? 0 : __float_as_int(p.w);
+    PairAcc<NT, ENERGY, Acc, MODE> acc;
+    for (int c = 0; c < 9; ++c) {
+      for (int k = kmin - 1; k <= kmax + 1; ++k) {
+        const int zc = (z0 - 1 + k + nz) % nz;
+        const uint32_t key = d.kbase[c] + (uint32_t)zc;
+        const float sz = k == 0 ? d.sz_lo : (k == nseg + 1 ? d.sz_hi : d.sz_mid);
+        if (c == 4)
+          global_range<NT, ENERGY, true, Acc, MODE>(b.rs, b.start[key], b.start[key + 1], xi, yi,
+                                                    zi, ti, d.sx[c], d.sy[c], sz, gh, d.lj, acc);
+        else
+          global_range<NT, ENERGY, false, Acc, MODE>(b.rs, b.start[key], b.start[key + 1], xi,
+                                                     yi, zi, ti, d.sx[c], d.sy[c], sz, 0, d.lj,
+                                                     acc);
+      }
+    }
+    if (valid) b.F[b.pid[gh]] = make_float4((float)acc.fx, (float)acc.fy, (float)acc.fz, 0.0f);
+    if (ENERGY) {
+      s[0] += warp_sum(valid ? (double)acc.pe : 0.0);
+      s[1] += warp_sum(valid ? (double)acc.pes : 0.0);
+      s[2] += warp_sum(valid ? (double)acc.vir : 0.0);
+      s[3] += (double)warp_sum(valid ? acc.n : 0u);
+    }
+  }
+  for (int k = 0; k < 4; ++k) ce[k] = s[k];
+}
+
+// ---- the kernel ---------------------------------------------------------------
+
+template <int NT, bool ENERGY, typename Acc, int kProd, int kCons, int MODE>
+__global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 1 : 2)
+    k_force(ForceBufs b) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ ItemDesc<NT> desc[2];
+  __shared__ Scratch sc;
+  __shared__ uint64_t full[2], empty[2], landed[2];
+  __shared__ double cle[2][kWinCap][4];
+  __shared__ int abort_flag, wait_ok;
+
+  const uint32_t slots = padded_slots((uint32_t)b.cap);
+  const uint32_t pbytes = plane_bytes(slots, NT), wbytes = warp_bytes(slots);
+  // stage buffer k (computed, not indexed, so it stays in registers)
+  auto planes = [&](int k) {
+    float *base = reinterpret_cast<float *>(smem_raw + (size_t)k * pbytes);
+    Planes p;
+    p.X = base;
+    p.Y = base + slots;
+    p.Z = base + 2 * slots;
+    p.T = NT > 1 ? reinterpret_cast<uint32_t *>(base + 3 * slots) : nullptr;
+    return p;
+  };
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 2; ++k) {
+      mbar_init(&full[k], 1);
+      mbar_init(&empty[k], kCons);
+      mbar_init(&landed[k], 1);
+    }
+    abort_flag = 0;
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const volatile int *abort_v = &abort_flag;
+
+  if (warp < kProd) {
+    // producers: wait for a free buffer (thread 0 polls; the group learns the
+    // outcome through its barrier), then stage the next item into it
+    auto wait_empty = [&](int bf, uint32_t parity) -> bool {
+      if (threadIdx.x == 0) {
+        const bool ok = mbar_wait_bounded(&empty[bf], parity);
+        wait_ok = ok;
+        if (!ok) {
+          atomicOr(&b.status[desc[bf].sys], kStatusWaitTimeout);
+          abort_flag = 1;
+        }
+      }
+      producer_sync<kProd>();
+      const bool ok = wait_ok;
+      producer_sync<kProd>();
+      return ok;
+    };
+    uint32_t lphase0 = 0u, lphase1 = 0u, running = 0;
+    uint32_t n = 0;
+    for (;; ++n) {
+      const uint32_t item = blockIdx.x + n * gridDim.x;
+      if (item >= b.nitems) break;
+      const int bf = n & 1;
+      if (n >= 2) {
+        // the consumers are done with item n - 2 in this buffer
+        if (!wait_empty(bf, ((n >> 1) - 1) & 1u)) return;
+        if (ENERGY && threadIdx.x == 0) write_partials(b, desc[bf], cle[bf]);
+        producer_sync<kProd>();
+      }
+      const bool ok = produce_item<NT, MODE, kProd, kCons>(
+          b, item, desc[bf], sc, planes(bf), &landed[bf], bf ? lphase1 : lphase0, running);
+      if (!ok) {
+        if (threadIdx.x == 0) abort_flag = 1;
+        return;
+      }
+      if (threadIdx.x == 0) mbar_arrive(&full[bf]);
+    }
+    // the last two items: wait for the consumers, then their energy partials
+    for (uint32_t m = n >= 2 ? n - 2 : 0; m < n; ++m) {
+      const int bf = m & 1;
+      if (!wait_empty(bf, (m >> 1) & 1u)) return;
+      if (ENERGY && threadIdx.x == 0) write_partials(b, desc[bf], cle[bf]);
+    }
+    return;
+  }
+
+  // consumers
+  const int cw = warp - kProd;
+  uint16_t *mylist =
+      reinterpret_cast<uint16_t *>(smem_raw + 2 * (size_t)pbytes + (size_t)cw * wbytes);
+  uint16_t *tb = mylist + 32 * kListLen;
+  for (uint32_t n = 0;; ++n) {
+    const uint32_t item = blockIdx.x + n * gridDim.x;
+    if (item >= b.nitems) break;
+    const int bf = n & 1;
+    bool ok = lane != 0 || mbar_wait_or_abort(&full[bf], (n >> 1) & 1u, abort_v);
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    if (!ok) {
+      if (lane == 0 && !*abort_v) atomicOr(&b.status[0], kStatusWaitTimeout);
+      return;
+    }
+    const ItemDesc<NT> &d = desc[bf];
+    const Planes pbuf = planes(bf);
+    if (!d.skip) {
+      if (!d.overflow) {
+        // clusters go round-robin over the CTA's whole item sequence
+        const uint32_t first = ((uint32_t)cw + (uint32_t)kCons - d.base) % (uint32_t)kCons;
+        for (uint32_t cl = first; cl < d.nclus; cl += kCons) {
+          double ce[4];
+          consume_cluster<NT, ENERGY, Acc, MODE>(b, d, pbuf, cl, mylist, tb, ce);
+          if (ENERGY && lane == 0)
+            for (int k = 0; k < 4; ++k) cle[bf][cl][k] = ce[k];
+        }
+      } else {
+        for (uint32_t t = (uint32_t)cw; t < d.ntask; t += kCons) {
+          double ce[4];
+          consume_task_global<NT, ENERGY, Acc, MODE>(b, d, t, ce);
+          if (ENERGY && lane == 0)
+            for (int k = 0; k < 4; ++k) cle[bf][t][k] = ce[k];
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[bf]);
+  }
+}
+
+// CTAs per SM of a launch shape, from the occupancy calculator.
+template <typename K>
+int resident_ctas(K kern, int threads, size_t smem) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem) != cudaSuccess) n = 1;
+  return n > 0 ? n : 1;
+}
+
+int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 1;
+  }
+  return n;
+}
+
+template <int NT, bool E, typename Acc, int P, int C, int MODE = kModeLJ>
 cudaError_t launch_w(const ForceBufs &b, cudaStream_t s) {
-  const size_t smem = smem_bytes((uint32_t)b.cap, W, NT);
-  auto kern = k_force<NT, E, Acc, W, MODE>;
+  const size_t smem = smem_bytes((uint32_t)b.cap, C, NT);
+  auto kern = k_force<NT, E, Acc, P, C, MODE>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  kern<<<b.nitems, W * 32, smem, s>>>(b);
+  // persistent grid: every resident CTA slot, at most one CTA per item
+  const long slots = (long)resident_ctas(kern, (P + C) * 32, smem) * sm_count();
+  const unsigned grid = (unsigned)std::min<long>(slots, (long)b.nitems);
+  kern<<<grid, (P + C) * 32, smem, s>>>(b);
   return cudaGetLastError();
 }
 
+// Launch shapes (producer warps, consumer warps): the default, and a small one.
+constexpr int kProdDefault = 4, kConsDefault = 8;
+constexpr int kProdSmall = 2, kConsSmall = 4;
+
 template <int NT, bool E, typename Acc>
-cudaError_t launch_t(const ForceBufs &b, int warps, cudaStream_t s) {
-  return warps == 4 ? launch_w<NT, E, Acc, 4>(b, s) : launch_w<NT, E, Acc, 8>(b, s);
+cudaError_t launch_t(const ForceBufs &b, int threads, cudaStream_t s) {
+  return threads == 128 ? launch_w<NT, E, Acc, kProdSmall, kConsSmall>(b, s)
+                        : launch_w<NT, E, Acc, kProdDefault, kConsDefault>(b, s);
 }
 
 template <int NT>
-cudaError_t launch_nt(const ForceBufs &b, bool energy, bool acc64, int warps, cudaStream_t s) {
+cudaError_t launch_nt(const ForceBufs &b, bool energy, bool acc64, int threads, cudaStream_t s) {
   if (energy) {
-    return acc64 ? launch_t<NT, true, double>(b, warps, s) : launch_t<NT, true, float>(b, warps, s);
+    return acc64 ? launch_t<NT, true, double>(b, threads, s)
+                 : launch_t<NT, true, float>(b, threads, s);
   }
-  return acc64 ? launch_t<NT, false, double>(b, warps, s) : launch_t<NT, false, float>(b, warps, s);
+  return acc64 ? launch_t<NT, false, double>(b, threads, s)
+               : launch_t<NT, false, float>(b, threads, s);
 }
 
 template <int MODE>
 cudaError_t launch_mode(const ForceBufs &b, int nt_max, cudaStream_t s) {
   if (b.nitems == 0) return cudaSuccess;
   switch (nt_max) {
-    case 1: return launch_w<1, false, float, kDefaultWarps, MODE>(b, s);
-    case 2: return launch_w<2, false, float, kDefaultWarps, MODE>(b, s);
-    case 3: case 4: return launch_w<4, false, float, kDefaultWarps, MODE>(b, s);
-    default: return launch_w<8, false, float, kDefaultWarps, MODE>(b, s);
+    case 1: return launch_w<1, false, float, kProdDefault, kConsDefault, MODE>(b, s);
+    case 2: return launch_w<2, false, float, kProdDefault, kConsDefault, MODE>(b, s);
+    case 3: case 4: return launch_w<4, false, float, kProdDefault, kConsDefault, MODE>(b, s);
+    default: return launch_w<8, false, float, kProdDefault, kConsDefault, MODE>(b, s);
   }
 }
 
@@ -740,12 +994,19 @@ cudaError_t launch_mode(const ForceBufs &b, int nt_max, cudaStream_t s) {
 int force_max_segment() { return kMaxSeg; }
 
 int force_max_capacity(int warps, int nt) {
-  // largest staged-atom capacity whose shared memory fits beside the static part
+  // largest staged-atom capacity whose shared memory fits one CTA
+  const int consumers = warps >= 8 ? kConsDefault : kConsSmall;
+  (void)kProdSmall;
   uint32_t cap = 64;
-  while (smem_bytes(cap + 64, warps, nt) <= 200u * 1024u) cap += 64;
+  while (smem_bytes(cap + 64, consumers, nt) <= 180u * 1024u) cap += 64;
   return (int)cap;
 }
-int force_threads() { return kDefaultWarps * 32; }
+
+int force_smem_per_cta(int cap, int nt) {
+  return (int)smem_bytes((uint32_t)cap, kConsDefault, nt) + 15 * 1024;
+}
+
+int force_threads() { return 256; }
 
 cudaError_t launch_force_capped(const ForceBufs &b, int nt_max, cudaStream_t s) {
   return launch_mode<kModeCapped>(b, nt_max, s);
@@ -758,12 +1019,11 @@ cudaError_t launch_force_softcore(const ForceBufs &b, int nt_max, cudaStream_t s
 cudaError_t launch_force(const ForceBufs &b, int nt_max, bool energy, bool acc64,
                          int block_threads, cudaStream_t s) {
   if (b.nitems == 0) return cudaSuccess;
-  const int warps = block_threads == 128 ? 4 : 8;
   switch (nt_max) {
-    case 1: return launch_nt<1>(b, energy, acc64, warps, s);
-    case 2: return launch_nt<2>(b, energy, acc64, warps, s);
-    case 3: case 4: return launch_nt<4>(b, energy, acc64, warps, s);
-    default: return launch_nt<8>(b, energy, acc64, warps, s);
+    case 1: return launch_nt<1>(b, energy, acc64, block_threads, s);
+    case 2: return launch_nt<2>(b, energy, acc64, block_threads, s);
+    case 3: case 4: return launch_nt<4>(b, energy, acc64, block_threads, s);
+    default: return launch_nt<8>(b, energy, acc64, block_threads, s);
   }
 }
 

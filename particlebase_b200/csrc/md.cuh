@@ -15,6 +15,8 @@
 //   pid    uint32[N]   particle id at each sorted slot (cudaCutoffBlock::pid)
 //   slot   uint32[N]   sorted slot of each particle (inverse of pid)
 //   rs     float4[N]   sorted positions, w = type id bits (cudaSortedPositions::r_s)
+//   xs, ys, zs float, ts uint32 [M]  SoA mirrors of rs; system s at mirror0(s) + k,
+//          mirror0 a multiple of 4 (M = sum of the systems' sizes rounded up to 4, + 4)
 // Cell keys order the (x, y) columns of a box along a Morton (Z-order) curve and
 // keep z fastest, so the three z-adjacent cells of a column are contiguous.
 #pragma once
@@ -33,6 +35,7 @@ struct SysDesc {
   uint32_t lj;              // index of this system's LJ table
   float dt;                 // time step
   uint32_t cap;             // staged-atom capacity of this system's force CTAs
+  uint32_t mirror0;         // first slot of this system in the SoA mirrors (multiple of 4)
 };
 
 // Work item of the force kernel: one (x, y) column of one system, z cells
@@ -59,11 +62,18 @@ struct CellBufs {
   uint32_t *key, *within, *count, *start, *tilesum;
   uint32_t *pid_tmp, *pid, *slot;
   float4 *rs;
+  // structure-of-arrays mirrors of rs (nullptr: not written); system s's
+  // sorted atom k sits at mirror0 + k, so 16-byte runs align the same way
+  // whether the system runs alone or in a batch
+  float *xs, *ys, *zs;
+  uint32_t *ts;
   uint32_t *status;
 };
 
 struct ForceBufs {
   const float4 *rs;
+  const float *xs, *ys, *zs;  // SoA mirrors of rs (per-system aligned, see CellBufs)
+  const uint32_t *ts;
   const uint32_t *start;     // packed cell starts
   const uint32_t *pid;
   const SysDesc *sys;

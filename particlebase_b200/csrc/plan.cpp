@@ -66,13 +66,17 @@ void neighbor_table(const Grid &g, std::vector<uint32_t> &out) {
       }
 }
 
-int choose_segment(double atoms_per_cell, int nz, double scale) {
-  // about 160 home atoms (20 clusters of 8) per force CTA; PB_FORCE_SEG overrides
+int choose_segment(double atoms_per_cell, int nz, double scale, int nt) {
+  // about 200 home atoms (25 clusters of 8) per force work item; PB_FORCE_SEG
+  // overrides.  Shorter runs while the stage would not let two force CTAs
+  // share an SM.
   const double apc = std::max(atoms_per_cell, 1.0);
-  int seg = (int)std::lround(160.0 * scale / apc);
+  int seg = (int)std::lround(200.0 * scale / apc);
   if (const char *e = std::getenv("PB_FORCE_SEG")) seg = std::atoi(e);
   seg = std::max(1, std::min(seg, force_max_segment()));
-  return std::min(seg, nz);
+  seg = std::min(seg, nz);
+  while (seg > 1 && force_smem_per_cta(choose_capacity(apc, seg), nt) > 112 * 1024) --seg;
+  return seg;
 }
 
 int choose_capacity(double atoms_per_cell, int seg) {

@@ -24,9 +24,10 @@ void morton_columns(int nx, int ny, std::vector<uint32_t> &rank, std::vector<uin
 // periodic, in reference cell numbering d2 + d1 nz + d0 nz ny.
 void neighbor_table(const Grid &g, std::vector<uint32_t> &out);
 
-// z cells per force work item for a mean cell occupancy: about 160 * scale
-// home atoms per CTA, at most kMaxSeg (see force.cu).
-int choose_segment(double atoms_per_cell, int nz, double scale = 1.0);
+// z cells per force work item for a mean cell occupancy: about 200 * scale
+// home atoms per item, at most force_max_segment(), and short enough for two
+// force CTAs per SM with `nt` atom types.
+int choose_segment(double atoms_per_cell, int nz, double scale = 1.0, int nt = 1);
 
 // Shared-memory capacity (atoms) of a force CTA staging 9 columns x (seg + 2)
 // cells at the given mean occupancy, with headroom for fluctuations.
@@ -41,5 +42,8 @@ void append_items(uint32_t sys, const Grid &g, int seg, uint32_t cell0,
 int force_max_segment();
 // Largest staged-atom capacity of a force CTA of `warps` warps for `nt` types.
 int force_max_capacity(int warps, int nt);
+// Shared memory (dynamic plus an upper bound of the static part) of one
+// default-shape force CTA with staged-atom capacity `cap` and `nt` types.
+int force_smem_per_cta(int cap, int nt);
 
 }  // namespace pb
