@@ -117,6 +117,8 @@ struct Scratch {
   uint32_t gstart[9][kMaxSeg + 3];
   uint32_t cnt[9][kMaxSeg + 3];
   uint32_t dst[27], lead[27], n[27], alen[27];
+  float shift[27][3];  // frame shift of each run
+  uint32_t shifted;    // runs with a nonzero shift (bit 3 c + p)
 };
 
 // One stage buffer: X, Y, Z planes and, with more than one type, a type plane.
@@ -371,6 +373,7 @@ __device__ bool produce_item(const ForceBufs &b, uint32_t item, ItemDesc<NT> &d,
   }
   const SysDesc &S = b.sys[it.sys];
   const Grid g = S.g;
+  const uint32_t mirror0 = S.mirror0, atom0 = S.atom0, scap = S.cap;
   const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
   const int z0 = it.z0, z1 = it.z1, nseg = z1 - z0;
   const int ncell = nseg + 2;  // staged cells per column
@@ -450,7 +453,7 @@ __device__ bool produce_item(const ForceBufs &b, uint32_t item, ItemDesc<NT> &d,
       const int k1 = p == 0 ? a_end : (p == 1 ? c_beg : ncell);
       n = d.off[c][k1] - d.off[c][k0];
       if (n > 0) {
-        m0 = S.mirror0 + (sc.gstart[c][k0] - S.atom0);
+        m0 = mirror0 + (sc.gstart[c][k0] - atom0);
         ma = m0 & ~3u;
         alen = ((m0 + n + 3u) & ~3u) - ma;
       }
@@ -463,15 +466,27 @@ __device__ bool produce_item(const ForceBufs &b, uint32_t item, ItemDesc<NT> &d,
     }
     const uint32_t dst = incl - alen;
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    // frame shift of each run: the column's x, y shift and the run's z shift
+    float rx = 0.f, ry = 0.f, rz = 0.f;
     if (lane < 27) {
+      const int c = lane / 3, pp = lane % 3;
+      rx = d.sx[c];
+      ry = d.sy[c];
+      rz = pp == 0 ? sz_lo : (pp == 1 ? Fz : sz_hi);
       sc.dst[lane] = dst;
       sc.lead[lane] = m0 - ma;
       sc.n[lane] = n;
       sc.alen[lane] = alen;
+      sc.shift[lane][0] = rx;
+      sc.shift[lane][1] = ry;
+      sc.shift[lane][2] = rz;
       if (lane % 3 == 0) d.ps[lane / 3] = dst;
     }
+    const uint32_t shifted =
+        __ballot_sync(0xffffffffu, n > 0 && (rx != 0.f || ry != 0.f || rz != 0.f));
+    if (lane == 0) sc.shifted = shifted;
     // the system's own capacity decides: the same path alone or batched
-    const bool overflow = total + 4u > padded_slots(S.cap) || nclus > (uint32_t)kWinCap;
+    const bool overflow = total + 4u > padded_slots(scap) || nclus > (uint32_t)kWinCap;
     if (lane == 0) {
       d.ps[9] = total;
       d.H = H;
@@ -511,12 +526,10 @@ __device__ bool produce_item(const ForceBufs &b, uint32_t item, ItemDesc<NT> &d,
     }
     producer_sync<kProd>();
     if (d.skip == 2) return false;
-    // frame shifts of the real atoms of each run
-    for (int p = 0; p < 27; ++p) {
-      const int c = p / 3, pp = p % 3;
-      const float sx = d.sx[c], sy = d.sy[c];
-      const float sz = pp == 0 ? sz_lo : (pp == 1 ? Fz : sz_hi);
-      if (sx == 0.f && sy == 0.f && sz == 0.f) continue;
+    // frame shifts of the real atoms of the shifted runs
+    for (uint32_t m = sc.shifted; m != 0u; m &= m - 1u) {
+      const int p = __ffs(m) - 1;
+      const float sx = sc.shift[p][0], sy = sc.shift[p][1], sz = sc.shift[p][2];
       const uint32_t s0 = sc.dst[p] + sc.lead[p], s1 = s0 + sc.n[p];
       for (uint32_t s = s0 + pt; s < s1; s += kPT) {
         pl.X[s] -= sx;
