@@ -149,6 +149,35 @@ __host__ __device__ __forceinline__ uint32_t smem_bytes(uint32_t cap, int consum
   return 2u * plane_bytes(slots, nt) + (uint32_t)consumers * warp_bytes(slots);
 }
 
+// Shared-memory access by 32-bit shared address.
+__device__ __forceinline__ float4 lds_f4(uint32_t a) {
+  float4 v;
+  // not volatile: the stage is read-only while a cluster is computed, so the
+  // compiler may schedule these loads freely
+  asm("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+      : "r"(a));
+  return v;
+}
+
+__device__ __forceinline__ float lds_f32(uint32_t a) {
+  float v;
+  asm("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+  return v;
+}
+
+// List entries are read after the warp's own stores (ordered by __syncwarp
+// and the memory clobber of those stores), so this load is volatile.
+__device__ __forceinline__ uint32_t lds_u16(uint32_t a) {
+  unsigned short v;
+  asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void sts_u16(uint32_t a, uint32_t v) {
+  asm volatile("st.shared.u16 [%0], %1;" ::"r"(a), "h"((unsigned short)v) : "memory");
+}
+
 // Position of flat quad u in a warp's quad table: within each chunk of 16,
 // the 4 quads lane q tests (u = q, q + 4, q + 8, q + 12) are adjacent, so a
 // lane fetches a chunk's quads with one 8-byte load.
@@ -160,11 +189,16 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Bounded wait that also gives up when the CTA has aborted.
+__device__ const int kNeverAbort = 0;
+
+// Bounded wait of the hand-off barriers: the polling thread sleeps between
+// polls (up to 1 us each, at most 2^22 polls), so waiting warps leave the
+// issue slots to the warps that compute.  Gives up early when the CTA has
+// aborted.
 __device__ __forceinline__ bool mbar_wait_or_abort(uint64_t *bar, uint32_t parity,
                                                    const volatile int *abort_flag) {
-  for (uint32_t it = 0; it < (1u << 24); ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
+  for (uint32_t it = 0; it < (1u << 22); ++it) {
+    if (mbar_try_wait_sleep(bar, parity, 1000u)) return true;
     if (*abort_flag) return false;
   }
   return false;
@@ -288,9 +322,12 @@ __device__ __forceinline__ void flush_packed(const float *X, const float *Y, con
   float2 s2 = make_float2(lj.s2[0], lj.s2[0]), e24 = make_float2(lj.e24[0], lj.e24[0]);
   float2 e4 = make_float2(lj.e4[0], lj.e4[0]), ush = make_float2(lj.ush[0], lj.ush[0]);
   float rc2a = lj.rc2[0], rc2b = lj.rc2[0];
+  // shared-memory byte addresses of the planes and of this lane's entries
+  const uint32_t xa = smem_u32(X), ya = smem_u32(Y), za = smem_u32(Z);
+  const uint32_t la = smem_u32(list) + 2u * (uint32_t)lane;
   for (uint32_t k = 0; k < cnt; k += 2) {
-    const uint32_t j0 = list[k * 32 + lane];
-    const uint32_t j1 = list[min(k + 1, cnt - 1) * 32 + lane];
+    const uint32_t j0 = lds_u16(la + 64u * k);
+    const uint32_t j1 = lds_u16(la + 64u * min(k + 1, cnt - 1));
     const bool v1 = k + 1 < cnt;
     if (NT > 1) {
       const int ka = ti * NT + (int)T[j0], kb = ti * NT + (int)T[j1];
@@ -303,9 +340,12 @@ __device__ __forceinline__ void flush_packed(const float *X, const float *Y, con
         ush = make_float2(lj.ush[ka], lj.ush[kb]);
       }
     }
-    const float2 dx = __ffma2_rn(make_float2(X[j0], X[j1]), m1, xi2);
-    const float2 dy = __ffma2_rn(make_float2(Y[j0], Y[j1]), m1, yi2);
-    const float2 dz = __ffma2_rn(make_float2(Z[j0], Z[j1]), m1, zi2);
+    const float2 dx =
+        __ffma2_rn(make_float2(lds_f32(xa + 4u * j0), lds_f32(xa + 4u * j1)), m1, xi2);
+    const float2 dy =
+        __ffma2_rn(make_float2(lds_f32(ya + 4u * j0), lds_f32(ya + 4u * j1)), m1, yi2);
+    const float2 dz =
+        __ffma2_rn(make_float2(lds_f32(za + 4u * j0), lds_f32(za + 4u * j1)), m1, zi2);
     const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
     const bool ina = r2.x < rc2a && r2.x > 0.0f;
     const bool inb = v1 && r2.y < rc2b && r2.y > 0.0f;
@@ -515,7 +555,7 @@ __device__ bool produce_item(const ForceBufs &b, uint32_t item, ItemDesc<NT> &d,
   if (d.overflow) return true;
   const uint32_t total = d.ps[9];
   if (total > 0) {
-    bool ok = pt != 0 || mbar_wait_bounded(landed, lphase);
+    bool ok = pt != 0 || mbar_wait_or_abort(landed, lphase, &kNeverAbort);
     lphase ^= 1u;
     // all producer threads learn the outcome through the barrier
     if (pt == 0 && !ok) {
@@ -675,22 +715,27 @@ __device__ __forceinline__ void consume_cluster(const ForceBufs &b, const ItemDe
     }
   };
   const float2 xi2 = make_float2(xi, xi), yi2 = make_float2(yi, yi), zi2 = make_float2(zi, zi);
-  uint16_t *out = mylist + lane;
+  // shared-memory byte addresses: candidate planes, and this lane's list
+  // entries at lbase + 64 k (entry k of lane `lane`)
+  const uint32_t xa = smem_u32(X), ya = smem_u32(Y), za = smem_u32(Z);
+  const uint32_t lbase = smem_u32(mylist) + 2u * (uint32_t)lane;
+  uint32_t o = 0;  // byte offset of this lane's next list entry
   // lane q tests quads u = q, q + 4, ... of the flat sequence, 4 per chunk; the
   // table pads the last chunk with the quad of far atoms
   for (uint32_t u0 = 0; u0 < Q; u0 += kChunk) {
-    const uint32_t cnt = (uint32_t)(out - (mylist + lane)) >> 5;
+    const uint32_t cnt = o >> 6;
     if (__reduce_max_sync(0xffffffffu, cnt) > (uint32_t)(kListLen - kChunk)) {
       flush(cnt);
       __syncwarp();
-      out = mylist + lane;
+      o = 0;
     }
     const uint2 qq = *reinterpret_cast<const uint2 *>(tb + u0 + 4 * q);
     const uint32_t quads[4] = {qq.x & 0xffffu, qq.x >> 16, qq.y & 0xffffu, qq.y >> 16};
 #pragma unroll
     for (int kk = 0; kk < kChunk / 4; ++kk) {
       const uint32_t quad = quads[kk];
-      const float4 x4 = X4[quad], y4 = Y4[quad], z4 = Z4[quad];
+      const float4 x4 = lds_f4(xa + quad * 16u), y4 = lds_f4(ya + quad * 16u),
+                   z4 = lds_f4(za + quad * 16u);
       const float2 dxa = __ffma2_rn(make_float2(x4.x, x4.y), m1, xi2);
       const float2 dxb = __ffma2_rn(make_float2(x4.z, x4.w), m1, xi2);
       const float2 dya = __ffma2_rn(make_float2(y4.x, y4.y), m1, yi2);
@@ -702,17 +747,17 @@ __device__ __forceinline__ void consume_cluster(const ForceBufs &b, const ItemDe
       // the stores are in bounds whether or not they are kept: the check above
       // leaves room for every candidate of this chunk
       const uint32_t s = quad * 4u;
-      out[0] = (uint16_t)s;
-      out += da.x < 0.0f ? 32 : 0;
-      out[0] = (uint16_t)(s + 1u);
-      out += da.y < 0.0f ? 32 : 0;
-      out[0] = (uint16_t)(s + 2u);
-      out += db.x < 0.0f ? 32 : 0;
-      out[0] = (uint16_t)(s + 3u);
-      out += db.y < 0.0f ? 32 : 0;
+      sts_u16(lbase + o, s);
+      o += da.x < 0.0f ? 64u : 0u;
+      sts_u16(lbase + o, s + 1u);
+      o += da.y < 0.0f ? 64u : 0u;
+      sts_u16(lbase + o, s + 2u);
+      o += db.x < 0.0f ? 64u : 0u;
+      sts_u16(lbase + o, s + 3u);
+      o += db.y < 0.0f ? 64u : 0u;
     }
   }
-  flush((uint32_t)(out - (mylist + lane)) >> 5);
+  flush(o >> 6);
   __syncwarp();
   float fx, fy, fz;
   Acc e0 = 0, e1 = 0, e2 = 0;
@@ -857,7 +902,7 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
     // outcome through its barrier), then stage the next item into it
     auto wait_empty = [&](int bf, uint32_t parity) -> bool {
       if (threadIdx.x == 0) {
-        const bool ok = mbar_wait_bounded(&empty[bf], parity);
+        const bool ok = mbar_wait_or_abort(&empty[bf], parity, &kNeverAbort);
         wait_ok = ok;
         if (!ok) {
           atomicOr(&b.status[desc[bf].sys], kStatusWaitTimeout);
