@@ -14,9 +14,10 @@ ranks.  With --gpus N > 1 (torchrun) every rank runs its own replica of the
 system (the path does not shard across GPUs: replicas only, weak scaling).
 
 `e2e` runs the reference driver loop through the public API with host
-buffers: import from host memory, then per step one pb_md_run call and a
-temperature read-back (as testMD2.cu:149-168 does), then the final positions
-copied back; wall-clock time.  `cpu_baseline` is the FP64 oracle (OpenMP,
+buffers over the workload's 500 steps: handle set-up and import from host
+memory, then per step one pb_md_run call and a temperature read-back (as
+testMD2.cu:149-168 does), then the final positions copied back; wall-clock
+time.  `cpu_baseline` is the FP64 oracle (OpenMP,
 all host cores) on a bounded sample of the same system.  `--impl reference`
 times the reference's own MD kernels compiled for the CPU (oracle/_ref), or the
 oracle port where that build is absent.
@@ -42,9 +43,11 @@ DT = 0.005
 METRIC = "LJ atom-steps/s at 1M atoms (Gaussian NVT, cell list rebuilt every step)"
 UNIT = "atom-steps/s"
 WORKLOAD = "lj_fcc_1048576_gauss_rho0.8442_T0.72_rc2.5"
+C2_STEPS = 500  # steps of the 1,048,576-atom Gaussian workload
 
 
 # --------------------------------------------------------------------------- utils
+
 
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -280,8 +283,9 @@ def run_ours(args, dist: Dist) -> dict:
     evolve_bytes = 60.0 * s.n
     traffic = profiled_traffic("k_force")
 
-    # e2e through the public API with host buffers (reference driver loop)
-    e2e_steps = max(4, min(steps, 50))
+    # e2e through the public API with host buffers (reference driver loop),
+    # over the workload's 500 steps (set-up and import included)
+    e2e_steps = C2_STEPS
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     q = from_system(s, gaussian=True, fp64_velocities=False)

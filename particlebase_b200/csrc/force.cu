@@ -731,8 +731,11 @@ __device__ __forceinline__ void consume_cluster(const ForceBufs &b, const ItemDe
     }
     const uint2 qq = *reinterpret_cast<const uint2 *>(tb + u0 + 4 * q);
     const uint32_t quads[4] = {qq.x & 0xffffu, qq.x >> 16, qq.y & 0xffffu, qq.y >> 16};
+    // steps of this chunk that hold a real quad for some lane (warp-uniform)
+    const uint32_t nsteps = min((Q - u0 + 3u) >> 2, (uint32_t)(kChunk / 4));
 #pragma unroll
     for (int kk = 0; kk < kChunk / 4; ++kk) {
+      if ((uint32_t)kk >= nsteps) break;
       const uint32_t quad = quads[kk];
       const float4 x4 = lds_f4(xa + quad * 16u), y4 = lds_f4(ya + quad * 16u),
                    z4 = lds_f4(za + quad * 16u);
