@@ -15,7 +15,7 @@
 //   k_bin       read r (16 B/atom), write key + within-cell ticket (8 B/atom)
 //   k_scan_*    exclusive scan of per-cell counts -> start[], zero the counts
 //   k_scatter   pid_tmp[start[key] + ticket] = i
-//   k_canon     one warp per cell: order members by (z, particle id), write
+//   k_canon     one warp per two cells: order members by (z, particle id), write
 //               pid, slot, the sorted position float4 (type id in .w) and its
 //               structure-of-arrays mirror (x, y, z, type) for the force kernel
 #include "md.cuh"
@@ -153,47 +153,70 @@ __device__ __forceinline__ bool canon_before(float za, uint32_t a, float zb, uin
   return za < zb || (za == zb && a < b);
 }
 
-// One warp per packed cell.  The rank of a member is the number of members
-// before it in (z, particle id) order, which orders each cell canonically
-// without depending on the atomic tickets of k_bin.
+// Rank of every member of one cell by (z, particle id), one lane per member,
+// among the `width` lanes starting at lane `base` (width 16 or 32).  The rank
+// of a member is the number of members before it in that order, which orders
+// each cell canonically without depending on the atomic tickets of k_bin.
+__device__ __forceinline__ void canon_cell(const CellBufs &b, uint32_t s0, uint32_t n, int li,
+                                           int base, uint32_t lanes_n) {
+  const uint32_t me = li < (int)n ? b.pid_tmp[s0 + li] : kNone;
+  const float4 p = li < (int)n ? b.r[me] : make_float4(0.f, 0.f, 0.f, 0.f);
+  uint32_t rank = 0;
+  for (uint32_t k = 0; k < lanes_n; ++k) {
+    const uint32_t other = __shfl_sync(0xffffffffu, me, base + (int)k);
+    const float zo = __shfl_sync(0xffffffffu, p.z, base + (int)k);
+    rank += (k < n && canon_before(zo, other, p.z, me)) ? 1u : 0u;
+  }
+  if (li < (int)n) {
+    const uint32_t s = s0 + rank;
+    b.pid[s] = me;
+    b.slot[me] = s;
+    b.rs[s] = make_float4(p.x, p.y, p.z, __int_as_float((int)b.type[me]));
+    if (b.xs) write_mirror(b, me, s, p);
+  }
+}
+
+// Cells with more than 32 members: O(n^2 / 32) ranking straight from global memory.
+__device__ void canon_large(const CellBufs &b, uint32_t s0, uint32_t n, int lane) {
+  for (uint32_t a = lane; a < n; a += 32) {
+    const uint32_t me = b.pid_tmp[s0 + a];
+    const float4 p = b.r[me];
+    uint32_t rank = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+      const uint32_t other = b.pid_tmp[s0 + k];
+      rank += canon_before(b.r[other].z, other, p.z, me) ? 1u : 0u;
+    }
+    const uint32_t s = s0 + rank;
+    b.pid[s] = me;
+    b.slot[me] = s;
+    b.rs[s] = make_float4(p.x, p.y, p.z, __int_as_float((int)b.type[me]));
+    if (b.xs) write_mirror(b, me, s, p);
+  }
+}
+
+// One warp per pair of packed cells: when both hold at most 16 members, each
+// half-warp orders one of them; otherwise the whole warp orders one, then the
+// other.
 __global__ void __launch_bounds__(256) k_canon(CellBufs b) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (warp >= b.ncells) return;
-  const uint32_t s0 = b.start[warp], s1 = b.start[warp + 1];
-  const uint32_t n = s1 - s0;
-  if (n <= 32) {
-    const uint32_t me = lane < (int)n ? b.pid_tmp[s0 + lane] : kNone;
-    const float4 p = lane < (int)n ? b.r[me] : make_float4(0.f, 0.f, 0.f, 0.f);
-    uint32_t rank = 0;
-    for (uint32_t k = 0; k < n; ++k) {
-      const uint32_t other = __shfl_sync(0xffffffffu, me, k);
-      const float zo = __shfl_sync(0xffffffffu, p.z, k);
-      rank += canon_before(zo, other, p.z, me) ? 1u : 0u;
-    }
-    if (lane < (int)n) {
-      const uint32_t s = s0 + rank;
-      b.pid[s] = me;
-      b.slot[me] = s;
-      b.rs[s] = make_float4(p.x, p.y, p.z, __int_as_float((int)b.type[me]));
-      if (b.xs) write_mirror(b, me, s, p);
-    }
-  } else {
-    // Large cells: O(n^2 / 32) ranking straight from global memory.
-    for (uint32_t a = lane; a < n; a += 32) {
-      const uint32_t me = b.pid_tmp[s0 + a];
-      const float4 p = b.r[me];
-      uint32_t rank = 0;
-      for (uint32_t k = 0; k < n; ++k) {
-        const uint32_t other = b.pid_tmp[s0 + k];
-        rank += canon_before(b.r[other].z, other, p.z, me) ? 1u : 0u;
-      }
-      const uint32_t s = s0 + rank;
-      b.pid[s] = me;
-      b.slot[me] = s;
-      b.rs[s] = make_float4(p.x, p.y, p.z, __int_as_float((int)b.type[me]));
-      if (b.xs) write_mirror(b, me, s, p);
-    }
+  const uint32_t c0 = 2 * warp;
+  if (c0 >= b.ncells) return;
+  const bool two = c0 + 1 < b.ncells;
+  const uint32_t s0 = b.start[c0], s1 = b.start[c0 + 1];
+  const uint32_t s2 = two ? b.start[c0 + 2] : s1;
+  const uint32_t n0 = s1 - s0, n1 = s2 - s1;
+  if (n0 <= 16 && n1 <= 16) {
+    const int half = lane >> 4;
+    canon_cell(b, half ? s1 : s0, half ? n1 : n0, lane & 15, half * 16, max(n0, n1));
+    return;
+  }
+  for (int k = 0; k < (two ? 2 : 1); ++k) {
+    const uint32_t sb = k ? s1 : s0, n = k ? n1 : n0;
+    if (n <= 32)
+      canon_cell(b, sb, n, lane, 0, n);
+    else
+      canon_large(b, sb, n, lane);
   }
 }
 
@@ -208,7 +231,7 @@ cudaError_t launch_cell_build(const CellBufs &b, cudaStream_t s) {
   k_scan_top<<<1, 1024, 0, s>>>(b, ntiles);
   k_scan_add<<<(b.ncells + 255) / 256, 256, 0, s>>>(b);
   k_scatter<<<nb, 256, 0, s>>>(b);
-  const uint64_t canon_threads = (uint64_t)b.ncells * 32;
+  const uint64_t canon_threads = (uint64_t)((b.ncells + 1) / 2) * 32;
   k_canon<<<(uint32_t)((canon_threads + 255) / 256), 256, 0, s>>>(b);
   return cudaGetLastError();
 }
