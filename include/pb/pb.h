@@ -100,6 +100,13 @@ int pb_md_destroy(pb_md *h);
 int pb_md_set_stream(pb_md *h, void *stream);
 const char *pb_md_last_error(const pb_md *h);
 /* Device status bits raised by kernels since the last call (cleared on read). */
+#define PB_STATUS_SMEM_OVERFLOW 0x1u   /* a force work item computed from global memory */
+#define PB_STATUS_NONFINITE 0x2u       /* a NaN or Inf reached a reduction */
+#define PB_STATUS_WAIT_TIMEOUT 0x4u    /* a bounded wait in a kernel gave up */
+#define PB_STATUS_CELL_OVERFLOW 0x8u   /* a cell held more atoms than a kernel supports */
+#define PB_STATUS_NOCONVERGE 0x10u     /* thermostat solve failed */
+#define PB_STATUS_NLIST_OVERFLOW 0x20u /* a neighbour-list row outgrew its capacity */
+#define PB_STATUS_STALE_NLIST 0x40u    /* an atom moved more than half the list skin */
 int pb_md_status(pb_md *h, uint32_t *bits);
 
 /* ---- set-up ---------------------------------------------------------------- */
@@ -154,6 +161,22 @@ int pb_md_wrap(pb_md *h);
 #define PB_MODE_VV 0
 #define PB_MODE_GAUSS 1
 int pb_md_run(pb_md *h, float dt, int mode, uint32_t steps);
+/* cudaParticleMD::useNList and the public field thickness
+ * (cudaParticleMD.hh:41, 167-179): force calls use a Verlet neighbour list of
+ * the atoms within rc + thickness (calcF_IJpairWithList_F4,
+ * kerneltemplate.hh:135-168), which only pb_md_make_nlist rebuilds; whole
+ * steps (pb_md_run) then skip the cell-list build, as testMD4n.cu:175-181 does.
+ * thickness < 0 turns the list off.  Single-system handles only.  A force call
+ * raises PB_STATUS_STALE_NLIST when an atom moved more than thickness / 2
+ * since the build. */
+int pb_md_use_nlist(pb_md *h, float thickness);
+/* cudaParticleMD::makeNList (cudaParticleMD.cu:338-394): rebuild the cell list
+ * and the neighbour list.  The cell edge (pb_md_setup_cells) must be at least
+ * rc + thickness, as the reference's cell blocks are; PB_ERR_ARG otherwise.
+ * Rows that outgrow their capacity are enlarged and the list built again. */
+int pb_md_make_nlist(pb_md *h);
+/* Mean and largest row length of the last list build, and the row capacity. */
+int pb_md_nlist_info(pb_md *h, double out[3]);
 /* pb_md_run bracketed by CUDA events on the handle's stream; *ms = elapsed. */
 int pb_md_run_timed(pb_md *h, float dt, int mode, uint32_t steps, float *ms);
 

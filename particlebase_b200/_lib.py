@@ -97,6 +97,9 @@ def _declare(L: C.CDLL) -> None:
         "pb_md_grid": [vp, C.POINTER(u32), C.POINTER(f32), C.POINTER(u32)],
         "pb_md_build_cells": [vp],
         "pb_md_force": [vp, u32],
+        "pb_md_use_nlist": [vp, f32],
+        "pb_md_make_nlist": [vp],
+        "pb_md_nlist_info": [vp, C.POINTER(f64)],
         "pb_md_clear_force": [vp],
         "pb_md_step_vv": [vp, f32],
         "pb_md_step_gauss": [vp, f32, f64],

@@ -17,6 +17,8 @@ enum StatusBits : uint32_t {
   kStatusWaitTimeout = 1u << 2,    // a bounded wait gave up
   kStatusCellOverflow = 1u << 3,   // a cell held more atoms than a kernel supports
   kStatusNoConverge = 1u << 4,     // thermostat solve failed
+  kStatusNlistOverflow = 1u << 5,  // a neighbour-list row outgrew its capacity
+  kStatusStaleList = 1u << 6,      // an atom moved more than half the list skin since the build
 };
 
 // Cell grid of one periodic box, bit-compatible with cudaCutoffBlock:

@@ -123,11 +123,60 @@ void free_cells(Engine &e) {
   e.cells_ready = false;
 }
 
+void free_nlist(Engine &e) {
+  dfree(e, e.nl_idx);
+  dfree(e, e.nl_cnt);
+  dfree(e, e.nl_atom);
+  dfree(e, e.nl_max);
+  dfree(e, e.nl_r0);
+  dfree(e, e.nl_partials);
+  dfree(e, e.d_nl_item0);
+  e.nl_cap = 0;
+  e.nl_built = false;
+}
+
+float max_rc2(const Engine &e) {
+  float m = 0.f;
+  const LJTable &T = e.sp[0].lj;
+  for (int k = 0; k < T.nt * T.nt; ++k) m = std::max(m, T.rc2[k]);
+  return m;
+}
+
+NlistBufs engine_nbufs(Engine &e) {
+  NlistBufs b{};
+  b.r = e.r;
+  b.rs = e.rs;
+  b.pid = e.pid;
+  b.start = e.start;
+  b.key = e.key;
+  b.colxy = e.colxy;
+  b.colrank = e.colrank;
+  b.type = e.type;
+  b.sys = e.d_sys;
+  b.lj = e.d_lj;
+  b.N = e.N;
+  b.cap = e.nl_cap;
+  const float rl = std::sqrt(max_rc2(e)) + e.nl_skin;
+  b.rl2 = rl * rl;
+  b.skin = e.nl_skin;
+  b.idx = e.nl_idx;
+  b.cnt = e.nl_cnt;
+  b.atom = e.nl_atom;
+  b.r0 = e.nl_r0;
+  b.maxcnt = e.nl_max;
+  b.F = e.F[e.cur];
+  b.partials = e.nl_partials;
+  b.status = e.status;
+  return b;
+}
+
 }  // namespace
 
 void engine_drop_graph(Engine &e) {
-  if (e.graph) cudaGraphExecDestroy(e.graph);
-  e.graph = nullptr;
+  for (auto &g : e.graph2) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
   for (auto &g : e.graph1) {
     if (g) cudaGraphExecDestroy(g);
     g = nullptr;
@@ -229,6 +278,7 @@ void engine_free(Engine &e) {
   dfree(e, e.d_fac);
   dfree(e, e.d_lj);
   dfree(e, e.steps_left);
+  free_nlist(e);
   if (e.own_stream && e.stream) cudaStreamDestroy(e.stream);
   e.stream = nullptr;
 }
@@ -349,6 +399,7 @@ int engine_import(Engine &e, uint32_t sys, const double *r3, const double *v3, c
 }
 
 int engine_setup_cells(Engine &e) {
+  e.nl_built = false;  // a list indexes the old sorted slots
   free_cells(e);
   engine_drop_graph(e);
   std::vector<uint32_t> rank_all, xy_all;
@@ -536,10 +587,116 @@ int engine_build(Engine &e) {
   return PB_OK;
 }
 
+int engine_use_nlist(Engine &e, float thickness) {
+  if (e.nsys != 1) return fail(e, PB_ERR_UNSUPPORTED, "neighbour lists are per single system");
+  engine_drop_graph(e);  // captured steps change with the force path
+  if (thickness < 0) {
+    e.nl_on = false;
+    free_nlist(e);
+    return PB_OK;
+  }
+  if (!(thickness < 1e30f)) return fail(e, PB_ERR_ARG, "bad thickness");
+  e.nl_on = true;
+  e.nl_skin = thickness;
+  e.nl_built = false;
+  return PB_OK;
+}
+
+int engine_make_nlist(Engine &e) {
+  if (!e.nl_on) return fail(e, PB_ERR_STATE, "neighbour list not in use");
+  if (!engine_ready(e)) return fail(e, PB_ERR_STATE, "need cell, LJ parameters and setup_cells");
+  const Grid &g = e.sp[0].grid;
+  const float rl = std::sqrt(max_rc2(e)) + e.nl_skin;
+  for (int k = 0; k < 3; ++k) {
+    // the 27-cell stencil must reach every pair within the list radius, as the
+    // reference's cell blocks (setupCutoffBlock(rc + thickness)) do
+    if (g.len[k] < rl) return fail(e, PB_ERR_ARG, "cell edge below cutoff + thickness");
+  }
+  const uint32_t N = e.N;
+  if (e.nl_cap == 0) {
+    // expected row length at the system's density, with headroom
+    const double vol = (double)g.L[0] * g.L[1] * g.L[2];
+    const double expect = N / vol * 4.18879020478639 * rl * rl * rl;
+    const uint32_t cap = ((uint32_t)(1.5 * expect) + 32u + 7u) & ~7u;
+    const uint32_t nb = nlist_blocks(N);
+    const uint32_t item0[2] = {0u, nb};
+    bool ok = dalloc(e, &e.nl_idx, (size_t)cap * N) == cudaSuccess &&
+              dalloc(e, &e.nl_cnt, N) == cudaSuccess && dalloc(e, &e.nl_atom, N) == cudaSuccess &&
+              dalloc(e, &e.nl_max, 1) == cudaSuccess && dalloc(e, &e.nl_r0, N) == cudaSuccess &&
+              dalloc(e, &e.nl_partials, (size_t)4 * nb) == cudaSuccess &&
+              dalloc(e, &e.d_nl_item0, 2) == cudaSuccess;
+    if (!ok) {
+      free_nlist(e);
+      return fail(e, PB_ERR_OOM, "neighbour list allocation failed");
+    }
+    E_CUDA(cudaMemcpyAsync(e.d_nl_item0, item0, sizeof(item0), cudaMemcpyHostToDevice, e.stream));
+    e.nl_cap = cap;
+    engine_drop_graph(e);  // captured steps hold the old buffers
+  }
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    int rc = engine_build(e);
+    if (rc) return rc;
+    E_CUDA(cudaMemsetAsync(e.nl_max, 0, sizeof(uint32_t), e.stream));
+    cudaError_t c = launch_nlist_build(engine_nbufs(e), e.stream);
+    if (c != cudaSuccess) return cuda_fail(e, c, "list build");
+    uint32_t mx = 0;
+    E_CUDA(cudaMemcpyAsync(&mx, e.nl_max, sizeof(mx), cudaMemcpyDeviceToHost, e.stream));
+    E_CUDA(cudaStreamSynchronize(e.stream));
+    if (mx <= e.nl_cap) {
+      e.nl_built = true;
+      return PB_OK;
+    }
+    // a row did not fit: grow the rows and build again (the overflow bit the
+    // build raised is cleared; the rebuilt list is complete)
+    dfree(e, e.nl_idx);
+    const uint32_t cap = (mx + mx / 4 + 7u) & ~7u;
+    if (dalloc(e, &e.nl_idx, (size_t)cap * N) != cudaSuccess) {
+      free_nlist(e);
+      return fail(e, PB_ERR_OOM, "neighbour list allocation failed");
+    }
+    e.nl_cap = cap;
+    engine_drop_graph(e);
+    std::vector<uint32_t> bits;
+    engine_status(e, bits);  // read and clear the overflow bit of the failed build
+  }
+  return fail(e, PB_ERR_DEVICE, "neighbour list rows still overflow");
+}
+
+int engine_nlist_info(Engine &e, double out[3]) {
+  if (!e.nl_on || !e.nl_built) return fail(e, PB_ERR_STATE, "no neighbour list");
+  std::vector<uint32_t> cnt(e.N);
+  E_CUDA(cudaMemcpyAsync(cnt.data(), e.nl_cnt, sizeof(uint32_t) * e.N, cudaMemcpyDeviceToHost,
+                         e.stream));
+  E_CUDA(cudaStreamSynchronize(e.stream));
+  double sum = 0;
+  uint32_t mx = 0;
+  for (uint32_t v : cnt) {
+    sum += v;
+    mx = std::max(mx, v);
+  }
+  out[0] = e.N ? sum / e.N : 0.0;
+  out[1] = mx;
+  out[2] = e.nl_cap;
+  return PB_OK;
+}
+
 int engine_force(Engine &e, bool energy) {
   if (!engine_ready(e)) return fail(e, PB_ERR_STATE, "need cell, LJ parameters and setup_cells");
   int nt = 1;
   for (const auto &P : e.sp) nt = std::max(nt, P.lj.nt);
+  if (e.nl_on) {
+    if (!e.nl_built) return fail(e, PB_ERR_STATE, "make the neighbour list first");
+    cudaError_t c = launch_nlist_force(engine_nbufs(e), nt, energy,
+                                       (e.flags & PB_MD_ACC_FP64) != 0, e.stream);
+    if (c != cudaSuccess) return cuda_fail(e, c, "list force");
+    e.last = e.cur;
+    if (energy) {
+      c = launch_energy_total(e.nl_partials, e.d_nl_item0, 1, e.sc, e.stream);
+      if (c != cudaSuccess) return cuda_fail(e, c, "energy total");
+    }
+    e.energy_valid = energy;
+    return PB_OK;
+  }
   cudaError_t c = launch_force(engine_fbufs(e), nt, energy, (e.flags & PB_MD_ACC_FP64) != 0,
                                e.force_threads, e.stream);
   if (c != cudaSuccess) return cuda_fail(e, c, "force");
@@ -574,7 +731,8 @@ int engine_wrap(Engine &e) {
 }
 
 int engine_step(Engine &e, int mode) {
-  int rc = engine_build(e);
+  // with a neighbour list the cell list is rebuilt only with the list
+  int rc = e.nl_on ? PB_OK : engine_build(e);
   if (!rc) rc = engine_force(e, false);
   if (!rc) rc = engine_evolve(e, mode, 1);
   return rc;
@@ -616,12 +774,13 @@ int engine_run(Engine &e, int mode, uint32_t steps) {
   };
   uint32_t done = 0;
   if (steps >= 2) {
-    if (!e.graph) {
-      const int rc = capture(2, &e.graph);
+    cudaGraphExec_t &g2 = e.graph2[e.cur];  // two steps return to this parity
+    if (!g2) {
+      const int rc = capture(2, &g2);
       if (rc) return rc;
     }
     for (; done + 2 <= steps; done += 2) {
-      E_CUDA(cudaGraphLaunch(e.graph, e.stream));
+      E_CUDA(cudaGraphLaunch(g2, e.stream));
       e.steps_done += 2;
       e.last = 1 - e.cur;  // two steps: cur is back where it was, F[1 - cur] is the newest
     }
@@ -649,7 +808,7 @@ int engine_profile(Engine &e, int mode, uint32_t steps, double ms[3]) {
   int rc = PB_OK;
   for (uint32_t k = 0; k < steps && !rc; ++k) {
     cudaEventRecord(ev[0], e.stream);
-    rc = engine_build(e);
+    rc = e.nl_on ? PB_OK : engine_build(e);
     cudaEventRecord(ev[1], e.stream);
     if (!rc) rc = engine_force(e, false);
     cudaEventRecord(ev[2], e.stream);

@@ -76,6 +76,16 @@ struct Engine {
   uint32_t cap_max = 0;
   bool energy_valid = false;
 
+  // Verlet neighbour list (single-system handles; see nlist.cu): while on,
+  // force calls use the list and whole steps skip the cell-list build
+  bool nl_on = false, nl_built = false;
+  float nl_skin = 0.f;
+  uint32_t nl_cap = 0;  // entries per row
+  uint32_t *nl_idx = nullptr, *nl_cnt = nullptr, *nl_atom = nullptr, *nl_max = nullptr;
+  float4 *nl_r0 = nullptr;
+  double *nl_partials = nullptr;
+  uint32_t *d_nl_item0 = nullptr;  // {0, blocks}: the list force's energy partials
+
   // per-system step budgets (serving): device counters, nullptr = no limits
   uint32_t *steps_left = nullptr;
   uint64_t steps_done = 0;           // time steps issued since creation
@@ -83,9 +93,10 @@ struct Engine {
   std::vector<uint64_t> budget_end;  // steps_done at which each budget runs out
   std::vector<int> last_at_set;      // `last` when each budget was set
 
-  // CUDA graph of two whole steps (the F ping-pong returns to its parity), and
-  // one-step graphs for each parity of the ping-pong
-  cudaGraphExec_t graph = nullptr;
+  // CUDA graphs of two whole steps and of one step, each for both parities of
+  // the F ping-pong: a captured step bakes in which buffer is F and which is
+  // Fold, so a graph only replays at the parity it was captured at
+  cudaGraphExec_t graph2[2] = {nullptr, nullptr};
   cudaGraphExec_t graph1[2] = {nullptr, nullptr};
   int graph_mode = -1;
   std::vector<float> graph_dt;
@@ -107,6 +118,12 @@ int engine_force(Engine &e, bool energy);
 int engine_evolve(Engine &e, int mode, int wrap);
 int engine_wrap(Engine &e);
 int engine_step(Engine &e, int mode);
+// Neighbour list: thickness >= 0 turns it on (rows within rc + thickness),
+// thickness < 0 off; make rebuilds the cell list and the neighbour list.
+int engine_use_nlist(Engine &e, float thickness);
+int engine_make_nlist(Engine &e);
+// Mean and largest row length of the last build, and the row capacity.
+int engine_nlist_info(Engine &e, double out[3]);
 int engine_run(Engine &e, int mode, uint32_t steps);
 int engine_profile(Engine &e, int mode, uint32_t steps, double ms[3]);
 int engine_clear_force(Engine &e);

@@ -90,6 +90,27 @@ struct ForceBufs {
   float sc_rc, sc_f0;          // soft-core force law: range and strength
 };
 
+// Verlet neighbour list of one system: row s holds the particles within the
+// list radius of the particle that sat in sorted slot s when the list was
+// built, column-major (entry k of row s at idx[k * N + s]).
+struct NlistBufs {
+  const float4 *r;           // positions, particle order
+  const float4 *rs;          // sorted positions (build)
+  const uint32_t *pid, *start, *key, *colxy, *colrank;  // cell list (build)
+  const uint16_t *type;
+  const SysDesc *sys;        // the one system
+  const LJTable *lj;
+  uint32_t N, cap;           // atoms; entries per row
+  float rl2;                 // list radius squared (build)
+  float skin;                // list radius minus the force cutoff
+  uint32_t *idx, *cnt, *atom;  // rows, row counts, particle of each row
+  float4 *r0;                // positions at the build, particle order
+  uint32_t *maxcnt;          // build: largest row count (reset by the caller)
+  float4 *F;                 // force output, particle order
+  double *partials;          // per-block energy partials (4 doubles per block)
+  uint32_t *status;
+};
+
 // Launchers (return cudaError_t of the launch).
 cudaError_t launch_cell_build(const CellBufs &b, cudaStream_t s);
 cudaError_t launch_force(const ForceBufs &b, int nt_max, bool energy, bool acc64,
@@ -98,5 +119,10 @@ cudaError_t launch_force(const ForceBufs &b, int nt_max, bool energy, bool acc64
 cudaError_t launch_force_capped(const ForceBufs &b, int nt_max, cudaStream_t s);
 // Soft-core force f0 cos(pi r / 2 sc_rc) along r (potentialSC), for annealing.
 cudaError_t launch_force_softcore(const ForceBufs &b, int nt_max, cudaStream_t s);
+// Neighbour list: build from the cell list; forces over the list.
+cudaError_t launch_nlist_build(const NlistBufs &b, cudaStream_t s);
+cudaError_t launch_nlist_force(const NlistBufs &b, int nt_max, bool energy, bool acc64,
+                               cudaStream_t s);
+uint32_t nlist_blocks(uint32_t N);  // blocks (energy partials) of launch_nlist_force
 
 }  // namespace pb

@@ -13,6 +13,14 @@
 using namespace pb;
 
 static_assert(sizeof(pb_particle) == 96, "pb_particle must match ParticleBase");
+static_assert(PB_STATUS_SMEM_OVERFLOW == pb::kStatusSmemOverflow &&
+                  PB_STATUS_NONFINITE == pb::kStatusNonFinite &&
+                  PB_STATUS_WAIT_TIMEOUT == pb::kStatusWaitTimeout &&
+                  PB_STATUS_CELL_OVERFLOW == pb::kStatusCellOverflow &&
+                  PB_STATUS_NOCONVERGE == pb::kStatusNoConverge &&
+                  PB_STATUS_NLIST_OVERFLOW == pb::kStatusNlistOverflow &&
+                  PB_STATUS_STALE_NLIST == pb::kStatusStaleList,
+              "status bits of the C ABI and the kernels");
 static_assert(offsetof(pb_particle, is_fixed) == 56, "pb_particle layout");
 static_assert(offsetof(pb_particle, a) == 64, "pb_particle layout");
 static_assert(offsetof(pb_particle, type) == 88, "pb_particle layout");
@@ -179,6 +187,17 @@ int pb_md_grid(const pb_md *h, uint32_t n3[3], float len3[3], uint32_t *ncells) 
 }
 
 int pb_md_build_cells(pb_md *h) { return h ? engine_build(h->e) : PB_ERR_ARG; }
+
+int pb_md_use_nlist(pb_md *h, float thickness) {
+  return h ? engine_use_nlist(h->e, thickness) : PB_ERR_ARG;
+}
+
+int pb_md_make_nlist(pb_md *h) { return h ? engine_make_nlist(h->e) : PB_ERR_ARG; }
+
+int pb_md_nlist_info(pb_md *h, double out[3]) {
+  if (!h || !out) return PB_ERR_ARG;
+  return engine_nlist_info(h->e, out);
+}
 
 int pb_md_force(pb_md *h, uint32_t flags) {
   return h ? engine_force(h->e, (flags & PB_FORCE_ENERGY) != 0) : PB_ERR_ARG;

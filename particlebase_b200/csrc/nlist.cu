@@ -1,0 +1,190 @@
+// Verlet neighbour list of one system.
+//
+// Replaces cudaParticleMD::makeNList (cudaParticleMD.cu:338-394: coordination
+// numbers, CSR row pointers, then makeJlist_WithBlock_F4 over the cell list)
+// and the list branch of cudaParticleMD::calcForce (cudaParticleMD.cu:41-44,
+// calcF_IJpairWithList_F4 at kerneltemplate.hh:135-168).  The list holds, for
+// every atom, the atoms within rc + thickness at the build; forces between
+// builds use the list instead of the cell list, and the cell list is rebuilt
+// only with the list, as testMD4n.cu:175-181 does.
+//
+// Layout.  Instead of CSR (a count pass, a scan and a fill pass), rows have a
+// fixed capacity and are stored column-major: entry k of row s at
+// idx[k * N + s], so the threads of a warp (consecutive rows) read one
+// coalesced line per entry.  Row s belongs to the atom that sat in sorted slot
+// s at the build, so a warp's atoms are neighbours of one another and their
+// partners' positions are mostly shared through L1.  The build reports the
+// longest row; the host grows the capacity and rebuilds when a row did not fit.
+//
+// Minimum image.  Each component of a pair difference is x_i - x_j, and when
+// that exceeds half the box the coordinate above the box middle is moved down
+// by L first, which is exact; the result is the minimum-image displacement
+// without the rounding of a large intermediate.
+//
+// Staleness.  The force kernel compares every atom's position with its
+// position at the build and raises kStatusStaleList when it moved more than
+// half the skin: the list may then miss a pair inside the cutoff.
+#include "md.cuh"
+
+namespace pb {
+namespace {
+
+constexpr int kNlThreads = 256;
+
+__device__ __forceinline__ float image_delta(float xi, float xj, float L, float hL) {
+  const float d = xi - xj;
+  if (d > hL) return (xi - L) - xj;
+  if (d < -hL) return xi - (xj - L);
+  return d;
+}
+
+__device__ __forceinline__ float round_image(float d, float L, float Linv) {
+  return d - L * rintf(d * Linv);
+}
+
+__global__ void __launch_bounds__(kNlThreads) k_nlist_build(NlistBufs b) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= b.N) return;
+  const SysDesc &S = b.sys[0];
+  const Grid g = S.g;
+  const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+  const float Lx = g.L[0], Ly = g.L[1], Lz = g.L[2];
+  const float iLx = 1.0f / Lx, iLy = 1.0f / Ly, iLz = 1.0f / Lz;
+  const uint32_t i = b.pid[s];
+  const float4 p = b.rs[s];
+  const uint32_t kk = b.key[i] - S.cell0;
+  const uint32_t rank = kk / (uint32_t)nz;
+  const int z = (int)(kk - rank * (uint32_t)nz);
+  const uint32_t xy = b.colxy[S.col0 + rank];
+  const int d0 = (int)(xy / (uint32_t)ny), d1 = (int)(xy % (uint32_t)ny);
+  uint32_t n = 0;
+  for (int a = -1; a <= 1; ++a) {
+    for (int c = -1; c <= 1; ++c) {
+      const int c0 = (d0 + a + nx) % nx, c1 = (d1 + c + ny) % ny;
+      const uint32_t rk = b.colrank[S.col0 + (uint32_t)(c0 * ny + c1)];
+      for (int e = -1; e <= 1; ++e) {
+        const uint32_t key2 = S.cell0 + rk * (uint32_t)nz + (uint32_t)((z + e + nz) % nz);
+        const uint32_t t1 = b.start[key2 + 1];
+        for (uint32_t t = b.start[key2]; t < t1; ++t) {
+          if (t == s) continue;
+          const float4 q = b.rs[t];
+          const float dx = round_image(q.x - p.x, Lx, iLx);
+          const float dy = round_image(q.y - p.y, Ly, iLy);
+          const float dz = round_image(q.z - p.z, Lz, iLz);
+          if (fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < b.rl2) {
+            if (n < b.cap) b.idx[(size_t)n * b.N + s] = b.pid[t];
+            ++n;
+          }
+        }
+      }
+    }
+  }
+  b.cnt[s] = n;
+  b.atom[s] = i;
+  b.r0[i] = make_float4(p.x, p.y, p.z, 0.0f);
+  if (n > b.cap) atomicOr(&b.status[0], kStatusNlistOverflow);
+  atomicMax(b.maxcnt, n);
+}
+
+template <int NT, bool ENERGY, typename Acc>
+__global__ void __launch_bounds__(kNlThreads) k_nlist_force(NlistBufs b) {
+  __shared__ float s2[NT * NT], e24[NT * NT], e4[NT * NT], rc2[NT * NT], ush[NT * NT];
+  __shared__ double red[4 * 32];
+  if (threadIdx.x < NT * NT) {
+    const LJTable &T = b.lj[0];
+    const int k = (threadIdx.x / NT) * T.nt + threadIdx.x % NT;
+    s2[threadIdx.x] = T.s2[k];
+    e24[threadIdx.x] = T.e24[k];
+    e4[threadIdx.x] = T.e4[k];
+    rc2[threadIdx.x] = T.rc2[k];
+    ush[threadIdx.x] = T.ushift[k];
+  }
+  __syncthreads();
+  const Grid g = b.sys[0].g;
+  const float Lx = g.L[0], Ly = g.L[1], Lz = g.L[2];
+  const float hx = 0.5f * Lx, hy = 0.5f * Ly, hz = 0.5f * Lz;
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  Acc pe = 0, pes = 0, vir = 0;
+  uint32_t npairs = 0;
+  if (s < b.N) {
+    const uint32_t i = b.atom[s];
+    const float4 p = b.r[i];
+    const int ti = NT == 1 ? 0 : (int)b.type[i];
+    const uint32_t n = min(b.cnt[s], b.cap);
+    Acc fx = 0, fy = 0, fz = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+      const uint32_t j = b.idx[(size_t)k * b.N + s];
+      const float4 q = b.r[j];
+      const float dx = image_delta(p.x, q.x, Lx, hx);
+      const float dy = image_delta(p.y, q.y, Ly, hy);
+      const float dz = image_delta(p.z, q.z, Lz, hz);
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      const int kk = NT == 1 ? 0 : ti * NT + (int)b.type[j];
+      if (r2 < rc2[kk]) {
+        const float inv = rcp_approx(r2);
+        const float sr2 = s2[kk] * inv;
+        const float sr6 = sr2 * sr2 * sr2;
+        const float f = e24[kk] * sr6 * fmaf(2.0f, sr6, -1.0f) * inv;
+        fx += (Acc)(f * dx);
+        fy += (Acc)(f * dy);
+        fz += (Acc)(f * dz);
+        if (ENERGY) {
+          const float u = e4[kk] * sr6 * (sr6 - 1.0f);
+          pe += (Acc)(0.5f * u);
+          pes += (Acc)(0.5f * (u - ush[kk]));
+          vir += (Acc)(0.5f * f * r2);
+          ++npairs;
+        }
+      }
+    }
+    b.F[i] = make_float4((float)fx, (float)fy, (float)fz, 0.0f);
+    // has the atom left the skin the list was built with?
+    const float4 p0 = b.r0[i];
+    const float ex = image_delta(p.x, p0.x, Lx, hx), ey = image_delta(p.y, p0.y, Ly, hy);
+    const float ez = image_delta(p.z, p0.z, Lz, hz);
+    if (fmaf(ex, ex, fmaf(ey, ey, ez * ez)) > 0.25f * b.skin * b.skin)
+      atomicOr(&b.status[0], kStatusStaleList);
+  }
+  if (ENERGY) {
+    double v[4] = {(double)pe, (double)pes, (double)vir, (double)npairs};
+    block_sum<4>(v, red);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < 4; ++k) b.partials[(size_t)blockIdx.x * 4 + k] = v[k];
+  }
+}
+
+template <int NT>
+cudaError_t launch_nt(const NlistBufs &b, bool energy, bool acc64, cudaStream_t s) {
+  const uint32_t nb = nlist_blocks(b.N);
+  if (energy) {
+    if (acc64) k_nlist_force<NT, true, double><<<nb, kNlThreads, 0, s>>>(b);
+    else k_nlist_force<NT, true, float><<<nb, kNlThreads, 0, s>>>(b);
+  } else {
+    if (acc64) k_nlist_force<NT, false, double><<<nb, kNlThreads, 0, s>>>(b);
+    else k_nlist_force<NT, false, float><<<nb, kNlThreads, 0, s>>>(b);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+uint32_t nlist_blocks(uint32_t N) { return (N + kNlThreads - 1) / kNlThreads; }
+
+cudaError_t launch_nlist_build(const NlistBufs &b, cudaStream_t s) {
+  if (b.N == 0) return cudaSuccess;
+  k_nlist_build<<<nlist_blocks(b.N), kNlThreads, 0, s>>>(b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_nlist_force(const NlistBufs &b, int nt_max, bool energy, bool acc64,
+                               cudaStream_t s) {
+  if (b.N == 0) return cudaSuccess;
+  switch (nt_max) {
+    case 1: return launch_nt<1>(b, energy, acc64, s);
+    case 2: return launch_nt<2>(b, energy, acc64, s);
+    case 3: case 4: return launch_nt<4>(b, energy, acc64, s);
+    default: return launch_nt<8>(b, energy, acc64, s);
+  }
+}
+
+}  // namespace pb

@@ -150,6 +150,22 @@ class MDSystem:
     def calcForce(self, energy: bool = False) -> None:
         self._ck(self.lib.pb_md_force(self.h, L.FORCE_ENERGY if energy else 0), "force")
 
+    def useNList(self, thickness: float) -> None:
+        """cudaParticleMD::useNList with `thickness` (cudaParticleMD.hh:167-179):
+        force calls use a Verlet list of the atoms within rc + thickness,
+        rebuilt by makeNList; thickness < 0 turns it off."""
+        self._ck(self.lib.pb_md_use_nlist(self.h, C.c_float(thickness)), "use_nlist")
+
+    def makeNList(self) -> None:
+        """cudaParticleMD::makeNList (cudaParticleMD.cu:338-394): cell list and
+        neighbour list rebuilt from the current positions."""
+        self._ck(self.lib.pb_md_make_nlist(self.h), "make_nlist")
+
+    def nlist_info(self) -> dict:
+        out = (C.c_double * 3)()
+        self._ck(self.lib.pb_md_nlist_info(self.h, out), "nlist_info")
+        return {"mean": out[0], "max": out[1], "capacity": out[2]}
+
     def clearForce(self) -> None:
         self._ck(self.lib.pb_md_clear_force(self.h), "clear_force")
 
@@ -276,8 +292,11 @@ class MDSystem:
 
 
 def from_system(s: LJSystem, gaussian: bool = False, fp64_velocities: bool | None = None,
-                fp64_forces: bool = False, per_pair_cutoff: bool | None = None) -> MDSystem:
-    """Build a ready-to-step MDSystem from a host LJSystem (reduced units)."""
+                fp64_forces: bool = False, per_pair_cutoff: bool | None = None,
+                cell_rmax: float | None = None) -> MDSystem:
+    """Build a ready-to-step MDSystem from a host LJSystem (reduced units).
+    Cells are at least `cell_rmax` wide (default: the cutoff; a neighbour list
+    needs cutoff + thickness)."""
     p = MDSystem(s.n, gaussian=gaussian, fp64_velocities=fp64_velocities, fp64_forces=fp64_forces)
     p.setCell(s.box)
     p.kB = 1.0
@@ -290,5 +309,5 @@ def from_system(s: LJSystem, gaussian: bool = False, fp64_velocities: bool | Non
     else:
         p.setLJparams(s.lj[..., :2].reshape(-1), nt)
     p.import_arrays(s.r, s.v, s.mass, s.types)
-    p.setupCutoffBlock(float(s.rc))
+    p.setupCutoffBlock(float(s.rc if cell_rmax is None else cell_rmax))
     return p

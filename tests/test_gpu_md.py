@@ -361,3 +361,22 @@ def test_minimize_matches_oracle(cuda_lib, po):
     p.calcForce(energy=True)
     assert p.status() == 0
     assert p.sums()["pe"] / s.n < -4.0  # the random start is far above zero
+
+
+@pytest.mark.parametrize("gaussian", [False, True])
+def test_runs_of_odd_length_match_one_run(cuda_lib, gaussian):
+    """Whole steps replay from CUDA graphs that bake in which force buffer is
+    F and which is Fold; runs of odd length flip that parity, and later runs
+    must still pick the graph captured at the current parity.  Pieces of
+    1, 2, 3 and 4 steps give the same bits as one run of 10."""
+    from particlebase_b200.md import from_system
+    s = perturbed(W.fcc_system(6, 0.8442, 0.72, seed=61), 0.05, 62)
+    a = from_system(s, gaussian=gaussian)
+    a.clearForce()
+    for k in (1, 2, 3, 4):
+        a.run(0.005, k)
+    b = from_system(s, gaussian=gaussian)
+    b.clearForce()
+    b.run(0.005, 10)
+    assert np.array_equal(a.get("r"), b.get("r"))
+    assert np.array_equal(a.get("F"), b.get("F"))
