@@ -38,7 +38,7 @@ class cudaParticleMD : public cudaParticleVV,
   real mv2 = 0.0;     // cached value of the last calcMV2()
   real kB = 1;        // Boltzmann constant in simulation units
   real rmax2 = 0;     // square of the LJ cutoff
-  real thickness = 0; // neighbour-list skin (the cell list is rebuilt every step)
+  real thickness = 0; // neighbour-list skin: list radius sqrt(rmax2) + thickness
 
   void setup(int n) override {
     cudaParticleBase::setup(n);
@@ -188,10 +188,18 @@ class cudaParticleMD : public cudaParticleVV,
     for (uint32_t i = 0; i < N; ++i) o << i << "\t" << (real)(m[i] * v2[i]) << std::endl;
   }
 
-  // Neighbour lists (cudaParticleMD.cu:338-394): every step rebuilds the cell
-  // list here, which gives the forces a Verlet list would give.
+  // Neighbour lists (cudaParticleMD.hh:167-179, cudaParticleMD.cu:338-394):
+  // useNList switches force calls to a Verlet list of the atoms within
+  // sqrt(rmax2) + thickness; makeNList rebuilds the cell list and that list,
+  // with the thickness set at the time of the call.
   void useNList(void) { useNlist = true; }
-  void makeNList(void) {}
+  void makeNList(void) {
+    if (!useNlist) return;
+    need("makeNList");
+    sync_params();
+    pb_shim::check(pb_md_use_nlist(h, thickness), "useNList", h);
+    pb_shim::check(pb_md_make_nlist(h), "makeNList", h);
+  }
 
   // checkpoint: frame, particle arrays, cell grid, kB, rmax2
   virtual void pb_save(std::ostream &o) const {
