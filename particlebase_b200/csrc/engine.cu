@@ -129,6 +129,7 @@ void free_nlist(Engine &e) {
   dfree(e, e.nl_atom);
   dfree(e, e.nl_max);
   dfree(e, e.nl_r0);
+  dfree(e, e.nl_rl);
   dfree(e, e.nl_partials);
   dfree(e, e.d_nl_item0);
   e.nl_cap = 0;
@@ -163,6 +164,7 @@ NlistBufs engine_nbufs(Engine &e) {
   b.cnt = e.nl_cnt;
   b.atom = e.nl_atom;
   b.r0 = e.nl_r0;
+  b.rl = e.nl_rl;
   b.maxcnt = e.nl_max;
   b.F = e.F[e.cur];
   b.partials = e.nl_partials;
@@ -623,6 +625,7 @@ int engine_make_nlist(Engine &e) {
     bool ok = dalloc(e, &e.nl_idx, (size_t)cap * N) == cudaSuccess &&
               dalloc(e, &e.nl_cnt, N) == cudaSuccess && dalloc(e, &e.nl_atom, N) == cudaSuccess &&
               dalloc(e, &e.nl_max, 1) == cudaSuccess && dalloc(e, &e.nl_r0, N) == cudaSuccess &&
+              dalloc(e, &e.nl_rl, N) == cudaSuccess &&
               dalloc(e, &e.nl_partials, (size_t)4 * nb) == cudaSuccess &&
               dalloc(e, &e.d_nl_item0, 2) == cudaSuccess;
     if (!ok) {

@@ -82,7 +82,7 @@ struct Engine {
   float nl_skin = 0.f;
   uint32_t nl_cap = 0;  // entries per row
   uint32_t *nl_idx = nullptr, *nl_cnt = nullptr, *nl_atom = nullptr, *nl_max = nullptr;
-  float4 *nl_r0 = nullptr;
+  float4 *nl_r0 = nullptr, *nl_rl = nullptr;
   double *nl_partials = nullptr;
   uint32_t *d_nl_item0 = nullptr;  // {0, blocks}: the list force's energy partials
 

@@ -701,9 +701,6 @@ __device__ __forceinline__ void consume_cluster(const ForceBufs &b, const ItemDe
   const float2 nrc = make_float2(-rcmax2 * (1.0f + 1.0f / 1024.0f),
                                  -rcmax2 * (1.0f + 1.0f / 1024.0f));
   const float2 m1 = make_float2(-1.0f, -1.0f);
-  const float4 *X4 = reinterpret_cast<const float4 *>(X);
-  const float4 *Y4 = reinterpret_cast<const float4 *>(Y);
-  const float4 *Z4 = reinterpret_cast<const float4 *>(Z);
   PairAcc<NT, ENERGY, Acc, MODE> acc;
   PairAcc2<ENERGY> acc2;
   auto flush = [&](uint32_t cnt) {

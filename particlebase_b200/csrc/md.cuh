@@ -90,9 +90,9 @@ struct ForceBufs {
   float sc_rc, sc_f0;          // soft-core force law: range and strength
 };
 
-// Verlet neighbour list of one system: row s holds the particles within the
-// list radius of the particle that sat in sorted slot s when the list was
-// built, column-major (entry k of row s at idx[k * N + s]).
+// Verlet neighbour list of one system: row s holds the build-time sorted
+// slots of the atoms within the list radius of the atom that sat in slot s
+// when the list was built, column-major (entry k of row s at idx[k * N + s]).
 struct NlistBufs {
   const float4 *r;           // positions, particle order
   const float4 *rs;          // sorted positions (build)
@@ -104,7 +104,8 @@ struct NlistBufs {
   float rl2;                 // list radius squared (build)
   float skin;                // list radius minus the force cutoff
   uint32_t *idx, *cnt, *atom;  // rows, row counts, particle of each row
-  float4 *r0;                // positions at the build, particle order
+  float4 *rl;                // current positions in row order (refreshed every force call)
+  float4 *r0;                // positions at the build, row order
   uint32_t *maxcnt;          // build: largest row count (reset by the caller)
   float4 *F;                 // force output, particle order
   double *partials;          // per-block energy partials (4 doubles per block)
@@ -121,6 +122,7 @@ cudaError_t launch_force_capped(const ForceBufs &b, int nt_max, cudaStream_t s);
 cudaError_t launch_force_softcore(const ForceBufs &b, int nt_max, cudaStream_t s);
 // Neighbour list: build from the cell list; forces over the list.
 cudaError_t launch_nlist_build(const NlistBufs &b, cudaStream_t s);
+// (launch_nlist_force refreshes rl from r before the pair loop)
 cudaError_t launch_nlist_force(const NlistBufs &b, int nt_max, bool energy, bool acc64,
                                cudaStream_t s);
 uint32_t nlist_blocks(uint32_t N);  // blocks (energy partials) of launch_nlist_force

@@ -12,9 +12,11 @@
 // fixed capacity and are stored column-major: entry k of row s at
 // idx[k * N + s], so the threads of a warp (consecutive rows) read one
 // coalesced line per entry.  Row s belongs to the atom that sat in sorted slot
-// s at the build, so a warp's atoms are neighbours of one another and their
-// partners' positions are mostly shared through L1.  The build reports the
-// longest row; the host grows the capacity and rebuilds when a row did not fit.
+// s at the build, and entries are build-time slots too: every force call first
+// copies the current positions into that order (rl), so a warp's atoms are
+// neighbours of one another and the positions they gather sit in a few nearby
+// lines, mostly shared through L1.  The build reports the longest row; the
+// host grows the capacity and rebuilds when a row did not fit.
 //
 // Minimum image.  Each component of a pair difference is x_i - x_j, and when
 // that exceeds half the box the coordinate above the box middle is moved down
@@ -64,16 +66,22 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_build(NlistBufs b) {
       const uint32_t rk = b.colrank[S.col0 + (uint32_t)(c0 * ny + c1)];
       for (int e = -1; e <= 1; ++e) {
         const uint32_t key2 = S.cell0 + rk * (uint32_t)nz + (uint32_t)((z + e + nz) % nz);
-        const uint32_t t1 = b.start[key2 + 1];
-        for (uint32_t t = b.start[key2]; t < t1; ++t) {
-          if (t == s) continue;
-          const float4 q = b.rs[t];
-          const float dx = round_image(q.x - p.x, Lx, iLx);
-          const float dy = round_image(q.y - p.y, Ly, iLy);
-          const float dz = round_image(q.z - p.z, Lz, iLz);
-          if (fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < b.rl2) {
-            if (n < b.cap) b.idx[(size_t)n * b.N + s] = b.pid[t];
-            ++n;
+        const uint32_t t0 = b.start[key2], t1 = b.start[key2 + 1];
+        // four candidates per pass, their loads issued together
+        for (uint32_t tb = t0; tb < t1; tb += 4) {
+          float4 q[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) q[u] = b.rs[min(tb + u, t1 - 1)];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const uint32_t t = tb + u;
+            const float dx = round_image(q[u].x - p.x, Lx, iLx);
+            const float dy = round_image(q[u].y - p.y, Ly, iLy);
+            const float dz = round_image(q[u].z - p.z, Lz, iLz);
+            if (t < t1 && t != s && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < b.rl2) {
+              if (n < b.cap) b.idx[(size_t)n * b.N + s] = t;
+              ++n;
+            }
           }
         }
       }
@@ -81,9 +89,19 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_build(NlistBufs b) {
   }
   b.cnt[s] = n;
   b.atom[s] = i;
-  b.r0[i] = make_float4(p.x, p.y, p.z, 0.0f);
+  b.r0[s] = make_float4(p.x, p.y, p.z, 0.0f);
   if (n > b.cap) atomicOr(&b.status[0], kStatusNlistOverflow);
   atomicMax(b.maxcnt, n);
+}
+
+// Current positions in row order, so the pair loop gathers from build-time
+// slots (type id bits in w, as in the sorted positions).
+__global__ void __launch_bounds__(kNlThreads) k_nlist_gather(NlistBufs b) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= b.N) return;
+  const uint32_t i = b.atom[s];
+  const float4 p = b.r[i];
+  b.rl[s] = make_float4(p.x, p.y, p.z, __int_as_float((int)b.type[i]));
 }
 
 template <int NT, bool ENERGY, typename Acc>
@@ -108,38 +126,50 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_force(NlistBufs b) {
   uint32_t npairs = 0;
   if (s < b.N) {
     const uint32_t i = b.atom[s];
-    const float4 p = b.r[i];
-    const int ti = NT == 1 ? 0 : (int)b.type[i];
+    const float4 p = b.rl[s];
+    const int ti = NT == 1 ? 0 : __float_as_int(p.w);
     const uint32_t n = min(b.cnt[s], b.cap);
     Acc fx = 0, fy = 0, fz = 0;
-    for (uint32_t k = 0; k < n; ++k) {
-      const uint32_t j = b.idx[(size_t)k * b.N + s];
-      const float4 q = b.r[j];
-      const float dx = image_delta(p.x, q.x, Lx, hx);
-      const float dy = image_delta(p.y, q.y, Ly, hy);
-      const float dz = image_delta(p.z, q.z, Lz, hz);
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      const int kk = NT == 1 ? 0 : ti * NT + (int)b.type[j];
-      if (r2 < rc2[kk]) {
-        const float inv = rcp_approx(r2);
-        const float sr2 = s2[kk] * inv;
-        const float sr6 = sr2 * sr2 * sr2;
-        const float f = e24[kk] * sr6 * fmaf(2.0f, sr6, -1.0f) * inv;
-        fx += (Acc)(f * dx);
-        fy += (Acc)(f * dy);
-        fz += (Acc)(f * dz);
-        if (ENERGY) {
-          const float u = e4[kk] * sr6 * (sr6 - 1.0f);
-          pe += (Acc)(0.5f * u);
-          pes += (Acc)(0.5f * (u - ush[kk]));
-          vir += (Acc)(0.5f * f * r2);
-          ++npairs;
+    // four entries per pass: their row reads, then their position gathers, are
+    // issued before any of them is used (memory-level parallelism)
+    constexpr int kU = 4;
+    for (uint32_t k0 = 0; k0 < n; k0 += kU) {
+      uint32_t t[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u)
+        t[u] = k0 + u < n ? __ldg(&b.idx[(size_t)(k0 + u) * b.N + s]) : s;
+      float4 q[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) q[u] = b.rl[t[u]];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const float dx = image_delta(p.x, q[u].x, Lx, hx);
+        const float dy = image_delta(p.y, q[u].y, Ly, hy);
+        const float dz = image_delta(p.z, q[u].z, Lz, hz);
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const int kk = NT == 1 ? 0 : ti * NT + __float_as_int(q[u].w);
+        // padding entries point at the atom itself: r2 = 0, never counted
+        if (r2 < rc2[kk] && r2 > 0.0f) {
+          const float inv = rcp_approx(r2);
+          const float sr2 = s2[kk] * inv;
+          const float sr6 = sr2 * sr2 * sr2;
+          const float f = e24[kk] * sr6 * fmaf(2.0f, sr6, -1.0f) * inv;
+          fx += (Acc)(f * dx);
+          fy += (Acc)(f * dy);
+          fz += (Acc)(f * dz);
+          if (ENERGY) {
+            const float u2 = e4[kk] * sr6 * (sr6 - 1.0f);
+            pe += (Acc)(0.5f * u2);
+            pes += (Acc)(0.5f * (u2 - ush[kk]));
+            vir += (Acc)(0.5f * f * r2);
+            ++npairs;
+          }
         }
       }
     }
     b.F[i] = make_float4((float)fx, (float)fy, (float)fz, 0.0f);
     // has the atom left the skin the list was built with?
-    const float4 p0 = b.r0[i];
+    const float4 p0 = b.r0[s];
     const float ex = image_delta(p.x, p0.x, Lx, hx), ey = image_delta(p.y, p0.y, Ly, hy);
     const float ez = image_delta(p.z, p0.z, Lz, hz);
     if (fmaf(ex, ex, fmaf(ey, ey, ez * ez)) > 0.25f * b.skin * b.skin)
@@ -156,6 +186,7 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_force(NlistBufs b) {
 template <int NT>
 cudaError_t launch_nt(const NlistBufs &b, bool energy, bool acc64, cudaStream_t s) {
   const uint32_t nb = nlist_blocks(b.N);
+  k_nlist_gather<<<nb, kNlThreads, 0, s>>>(b);
   if (energy) {
     if (acc64) k_nlist_force<NT, true, double><<<nb, kNlThreads, 0, s>>>(b);
     else k_nlist_force<NT, true, float><<<nb, kNlThreads, 0, s>>>(b);
