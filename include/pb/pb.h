@@ -177,6 +177,16 @@ int pb_md_use_nlist(pb_md *h, float thickness);
 int pb_md_make_nlist(pb_md *h);
 /* Mean and largest row length of the last list build, and the row capacity. */
 int pb_md_nlist_info(pb_md *h, double out[3]);
+/* cudaCalcGR::setup + calcgr (cudaCalcGR.hh:27-40, cudaCalcGR.cu:85-116,
+ * calcGR_F4 at kernelinline.hh:433-449): counts of the unordered pairs of the
+ * handle's current positions per distance bin, minimum image, bin
+ * j = trunc(r / rstep + 1/2) counted when 0 < j < rnum, rnum = trunc(rmax /
+ * rstep) by the reference's FP32 rule.  All pairs, as the reference's pair
+ * list over every cell-block pair.  Call with counts = NULL to get *rnum, then
+ * with counts[*rnum] (overwritten; bin 0 stays 0).  rnum <= 16384.
+ * cudaCalcGR::igr2gr's normalisation g_j = counts_j * Q / (4 j^2 + 1/3),
+ * Q = 2 V / (N^2 pi rstep^3), is left to the caller (the drop-in class does it). */
+int pb_md_gr(pb_md *h, float rstep, float rmax, uint64_t *counts, uint32_t *rnum);
 /* pb_md_run bracketed by CUDA events on the handle's stream; *ms = elapsed. */
 int pb_md_run_timed(pb_md *h, float dt, int mode, uint32_t steps, float *ms);
 

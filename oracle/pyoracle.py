@@ -114,6 +114,8 @@ def ref() -> C.CDLL:
         L.ref_get_cells.argtypes = [C.c_void_p, _u32p, _u32p, _u32p]
         L.ref_get_neighbors.argtypes = [C.c_void_p, _u32p]
         L.ref_threads.restype = C.c_int
+        L.ref_gr.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_uint32]
+        L.ref_gr.restype = C.c_int
         _ref = L
     return _ref
 
@@ -305,8 +307,79 @@ class RefKernels:
         ref().ref_get_cells(self.h, bid, pid, bindex)
         return bid, pid, bindex
 
+    def gr_counts(self, rstep, rmax):
+        """cudaCalcGR pair counts per bin (after calc_block_id), from the
+        reference's own kernel; bin 0 holds nothing."""
+        L = ref()
+        rnum = L.ref_gr(self.h, rstep, rmax, None, 0)
+        out = np.zeros(rnum, np.uint32)
+        L.ref_gr(self.h, rstep, rmax, out.ctypes.data_as(C.c_void_p), rnum)
+        return out
+
     def neighbors(self):
         nc = ref().ref_num_cells(self.h)
         out = np.zeros(nc * 27, np.uint32)
         ref().ref_get_neighbors(self.h, out)
         return out.reshape(-1, 27)
+
+
+# ---- g(r) -------------------------------------------------------------------
+
+
+def gr_bins(rstep, rmax):
+    """Number of bins of cudaCalcGR::setup (cudaCalcGR.hh:27-31): rstepinv =
+    1 / rstep (double quotient stored as FP32), rnum = trunc(rmax * rstepinv)
+    in FP32."""
+    inv = np.float32(1.0 / np.float64(np.float32(rstep)))
+    return int(np.float32(np.float32(rmax) * inv)), inv
+
+
+def _image_delta32(a, b, L):
+    """x_i - x_j in FP32 with the minimum image, the coordinate above the box
+    middle moved down by L first (exact), as the CUDA g(r) and neighbour-list
+    kernels do."""
+    L = np.float32(L)
+    h = np.float32(0.5) * L
+    d = (a - b).astype(np.float32)
+    hi = d > h
+    lo = d < -h
+    d = np.where(hi, (a - L) - b, d)
+    d = np.where(lo, a - (b - L), d)
+    return d.astype(np.float32)
+
+
+def gr_counts(r4, box, rstep, rmax):
+    """Pair counts per bin of every unordered pair (i < j) of positions r4,
+    restating cudaCalcGR::calcgr with calcGR_F4 (kernelinline.hh:433-449):
+    bin = trunc(sqrt(r^2) * rstepinv + 0.5), counted when 0 < bin < rnum.
+    Arithmetic in FP32 without fused multiply-adds, r^2 = (dx^2 + dy^2) + dz^2,
+    with the exact minimum image of _image_delta32, as the CUDA kernel does
+    (the reference takes the minimum image inside r^2, distance2p at
+    kernelinline.hh:47-62, which can move a pair on a bin edge by one bin)."""
+    rnum, inv = gr_bins(rstep, rmax)
+    b = np.asarray(box, np.float32)
+    r = np.asarray(r4, np.float32)[:, :3]
+    n = len(r)
+    counts = np.zeros(rnum, np.int64)
+    Ls = [b[1] - b[0], b[3] - b[2], b[5] - b[4]]
+    for i0 in range(0, n, 512):
+        ri = r[i0:i0 + 512]
+        d = [_image_delta32(ri[:, None, k], r[None, :, k], Ls[k]) for k in range(3)]
+        r2 = ((d[0] * d[0] + d[1] * d[1]).astype(np.float32) + d[2] * d[2]).astype(np.float32)
+        bins = (np.sqrt(r2).astype(np.float32) * inv + np.float32(0.5)).astype(np.float32)
+        bins = np.floor(bins).astype(np.int64)
+        ii = np.arange(i0, i0 + len(ri))[:, None]
+        jj = np.arange(n)[None, :]
+        keep = (jj > ii) & (bins > 0) & (bins < rnum)
+        counts += np.bincount(bins[keep], minlength=rnum)[:rnum]
+    return counts
+
+
+def gr_normalise(counts, n, volume, rstep):
+    """cudaCalcGR::igr2gr (cudaCalcGR.cu:118-136): g_j = counts_j * Q /
+    (4 j^2 + 1/3), Q = 2 / N / (pi rstep^3) * V / N; g_0 = 0."""
+    j = np.arange(len(counts), dtype=np.float64)
+    q = 2.0 / n / (np.pi * rstep ** 3) * volume / n
+    g = counts * q / (4 * j * j + 1.0 / 3.0)
+    g[0] = 0.0
+    return g

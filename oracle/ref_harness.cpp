@@ -391,3 +391,52 @@ void ref_get_neighbors(void *h, uint32_t *out) {
 int ref_threads(void) { return omp_get_max_threads(); }
 
 }  // extern "C"
+
+extern "C" {
+
+// cudaCalcGR (cudaCalcGR.hh:27-40, cudaCalcGR.cu:52-116) on the CPU: the bin
+// count rule of setup(), the pair chunks of makePairInfo() (every pair of
+// occupied cell blocks I <= J, in chunks of at most 64 atoms), and the
+// reference's own calcF_IJpairWithBlock5_F4 kernel with calcGR_F4
+// (kerneltemplate.hh:423-512, kernelinline.hh:433-449) run as one block.
+// Needs ref_calc_block_id first.  Returns rnum; fills counts[rnum] when
+// counts is non-null and ncounts >= rnum (bin 0 holds nothing).
+int ref_gr(void *h, float rstep, float rmax, uint32_t *counts, uint32_t ncounts) {
+  RefSys &s = *(RefSys *)h;
+  const real rstepinv = 1.0 / rstep;
+  const uint32_t rnum = static_cast<uint32_t>(rmax * rstepinv);
+  if (!counts) return (int)rnum;
+  if (ncounts < rnum) return -1;
+  std::vector<uint4> info;
+  const std::vector<uint32_t> &bi = s.bindex;
+  auto block_end = [&](uint32_t I) {
+    uint32_t k = I + 1;
+    while (bi[k] == UINT_MAX) ++k;
+    return bi[k];
+  };
+  for (uint32_t I = 0; I < s.totalNumBlock; ++I) {
+    if (bi[I] == UINT_MAX) continue;
+    const uint32_t i0 = bi[I], i1 = block_end(I);
+    for (uint32_t J = I; J < s.totalNumBlock; ++J) {
+      if (bi[J] == UINT_MAX) continue;
+      const uint32_t j0 = bi[J], j1 = block_end(J);
+      for (uint32_t i = i0; i < i1; i += 64)
+        for (uint32_t j = j0; j < j1; j += 64)
+          info.push_back(uint4{i, std::min(i + 64, i1), j, std::min(j + 64, j1)});
+    }
+  }
+  calcGR_F4 P;
+  P.cx = s.cell[6];
+  P.cy = s.cell[7];
+  P.cz = s.cell[8];
+  P.rstepinv = rstepinv;
+  P.rnum = rnum;
+  P.typeID = nullptr;
+  std::vector<uint32_t> igr(rnum, 0);
+  launch(dim3(1), false, calcF_IJpairWithBlock5_F4<calcGR_F4>, P, s.r_s.data(), info.data(),
+         (uint32_t)info.size(), igr.data(), rnum);
+  for (uint32_t k = 0; k < rnum; ++k) counts[k] = igr[k];
+  return (int)rnum;
+}
+
+}  // extern "C"

@@ -100,6 +100,7 @@ def _declare(L: C.CDLL) -> None:
         "pb_md_use_nlist": [vp, f32],
         "pb_md_make_nlist": [vp],
         "pb_md_nlist_info": [vp, C.POINTER(f64)],
+        "pb_md_gr": [vp, f32, f32, vp, C.POINTER(u32)],
         "pb_md_clear_force": [vp],
         "pb_md_step_vv": [vp, f32],
         "pb_md_step_gauss": [vp, f32, f64],

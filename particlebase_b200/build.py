@@ -112,7 +112,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 SHIM = os.path.join(PKG, "shim")
 DRIVERS = os.path.join(SHIM, "_drivers")
-MD_DRIVERS = ("testMD1", "testMD2", "testMD3", "testMD4", "testMD4n")
+MD_DRIVERS = ("testMD1", "testMD2", "testMD3", "testMD4", "testMD4n", "calcgr1")
 
 
 def reference_dir() -> str:

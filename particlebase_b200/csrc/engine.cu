@@ -683,6 +683,31 @@ int engine_nlist_info(Engine &e, double out[3]) {
   return PB_OK;
 }
 
+int engine_gr(Engine &e, float rstep, float rmax, uint64_t *counts, uint32_t *rnum) {
+  if (e.nsys != 1) return fail(e, PB_ERR_UNSUPPORTED, "g(r) is per single system");
+  if (!(rstep > 0) || !(rmax > 0) || !rnum) return fail(e, PB_ERR_ARG, "bad g(r) bins");
+  if (!e.sp[0].cell_set) return fail(e, PB_ERR_STATE, "set the cell first");
+  // cudaCalcGR::setup (cudaCalcGR.hh:27-31): rstepinv = 1 / rstep as a double
+  // quotient stored in FP32, rnum = trunc(rmax * rstepinv) in FP32
+  const float inv = (float)(1.0 / (double)rstep);
+  const uint32_t n = (uint32_t)(rmax * inv);
+  *rnum = n;
+  if (!counts) return PB_OK;
+  if (n > gr_max_bins()) return fail(e, PB_ERR_ARG, "more g(r) bins than supported");
+  const float *c = e.sp[0].cell;
+  const float L[3] = {c[1] - c[0], c[3] - c[2], c[5] - c[4]};
+  unsigned long long *d = nullptr;
+  if (dalloc(e, &d, n) != cudaSuccess) return fail(e, PB_ERR_OOM, "g(r) counts");
+  cudaError_t st = cudaMemsetAsync(d, 0, sizeof(unsigned long long) * n, e.stream);
+  if (st == cudaSuccess) st = launch_gr(e.r, e.N, L, inv, n, d, e.stream);
+  if (st == cudaSuccess)
+    st = cudaMemcpyAsync(counts, d, sizeof(uint64_t) * n, cudaMemcpyDeviceToHost, e.stream);
+  dfree(e, d);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e.stream);
+  if (st != cudaSuccess) return cuda_fail(e, st, "g(r)");
+  return PB_OK;
+}
+
 int engine_force(Engine &e, bool energy) {
   if (!engine_ready(e)) return fail(e, PB_ERR_STATE, "need cell, LJ parameters and setup_cells");
   int nt = 1;

@@ -124,6 +124,9 @@ int engine_use_nlist(Engine &e, float thickness);
 int engine_make_nlist(Engine &e);
 // Mean and largest row length of the last build, and the row capacity.
 int engine_nlist_info(Engine &e, double out[3]);
+// Pair counts per distance bin of the current positions (single system);
+// *rnum = the bin count of the reference's rule; counts (host) when non-null.
+int engine_gr(Engine &e, float rstep, float rmax, uint64_t *counts, uint32_t *rnum);
 int engine_run(Engine &e, int mode, uint32_t steps);
 int engine_profile(Engine &e, int mode, uint32_t steps, double ms[3]);
 int engine_clear_force(Engine &e);

@@ -126,5 +126,10 @@ cudaError_t launch_nlist_build(const NlistBufs &b, cudaStream_t s);
 cudaError_t launch_nlist_force(const NlistBufs &b, int nt_max, bool energy, bool acc64,
                                cudaStream_t s);
 uint32_t nlist_blocks(uint32_t N);  // blocks (energy partials) of launch_nlist_force
+// Pair counts per distance bin over all unordered pairs (g(r)); counts must
+// be zeroed by the caller; rnum <= gr_max_bins().
+cudaError_t launch_gr(const float4 *r, uint32_t N, const float L[3], float inv, uint32_t rnum,
+                      unsigned long long *counts, cudaStream_t s);
+uint32_t gr_max_bins();
 
 }  // namespace pb

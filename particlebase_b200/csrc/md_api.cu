@@ -199,6 +199,10 @@ int pb_md_nlist_info(pb_md *h, double out[3]) {
   return engine_nlist_info(h->e, out);
 }
 
+int pb_md_gr(pb_md *h, float rstep, float rmax, uint64_t *counts, uint32_t *rnum) {
+  return h ? engine_gr(h->e, rstep, rmax, counts, rnum) : PB_ERR_ARG;
+}
+
 int pb_md_force(pb_md *h, uint32_t flags) {
   return h ? engine_force(h->e, (flags & PB_FORCE_ENERGY) != 0) : PB_ERR_ARG;
 }

@@ -166,6 +166,17 @@ class MDSystem:
         self._ck(self.lib.pb_md_nlist_info(self.h, out), "nlist_info")
         return {"mean": out[0], "max": out[1], "capacity": out[2]}
 
+    def gr_counts(self, rstep: float, rmax: float) -> np.ndarray:
+        """cudaCalcGR::calcgr: counts of the unordered pairs of the current
+        positions per distance bin (bin j = round(r / rstep), 0 < j < rnum)."""
+        n = C.c_uint32()
+        self._ck(self.lib.pb_md_gr(self.h, C.c_float(rstep), C.c_float(rmax), None,
+                                   C.byref(n)), "gr")
+        out = np.zeros(n.value, np.uint64)
+        self._ck(self.lib.pb_md_gr(self.h, C.c_float(rstep), C.c_float(rmax),
+                                   out.ctypes.data_as(C.c_void_p), C.byref(n)), "gr")
+        return out
+
     def clearForce(self) -> None:
         self._ck(self.lib.pb_md_clear_force(self.h), "clear_force")
 

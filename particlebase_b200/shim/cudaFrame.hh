@@ -67,6 +67,9 @@ class cudaFrame {
     }
   }
 
+  // the box as setCell stored it: xmin, xmax, ymin, ymax, zmin, zmax, (L/2)^2 x 3
+  const real *cellData(void) const { return cell; }
+
   virtual std::string additionalTag(void) const { return ""; }
   virtual std::string additionalOutput(uint32_t) const { return ""; }
 

@@ -134,6 +134,20 @@ def main() -> None:
     out["quirk_r"] = rr
     out["quirk_F"] = Rq.get4("F")
 
+    # 9. g(r): pair counts per bin from the reference's calcF_IJpairWithBlock5_F4
+    # with calcGR_F4 (cudaCalcGR), 500 fcc atoms perturbed by 0.2 sigma, bins of
+    # 0.05 sigma up to 4 sigma (just under half the 8.4-sigma box)
+    sg = W.fcc_system(5, 0.8442, 0.72, seed=3)
+    rng = np.random.default_rng(4)
+    rg = np.mod(sg.r + rng.uniform(-0.2, 0.2, sg.r.shape), sg.L).astype(np.float32).astype(
+        np.float64)
+    Rg = ref_system(sg, rg)
+    Rg.calc_block_id()
+    out["gr_box"] = sg.box
+    out["gr_r4"] = Rg.get4("r")
+    out["gr_rstep_rmax"] = np.array([0.05, 4.0], np.float32)
+    out["gr_counts"] = Rg.gr_counts(0.05, 4.0)
+
     path = os.path.join(HERE, "reference_kernels.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes")

@@ -239,3 +239,15 @@ def test_kob_andersen_forces_vs_reference_kernel(po):
     F = O2.get("F")
     Fr = R.get4("F")[:, :3].astype(np.float64)
     assert relrms(Fr, F) < 2e-4
+
+
+def test_gr_counts_match_reference_kernel(po, golden):
+    """The oracle's g(r) pair counts equal those of the reference's own
+    calcF_IJpairWithBlock5_F4 / calcGR_F4 kernel (golden fixture) bin for bin."""
+    rstep, rmax = (float(x) for x in golden["gr_rstep_rmax"])
+    counts = po.gr_counts(golden["gr_r4"], golden["gr_box"], rstep, rmax)
+    assert np.array_equal(counts, golden["gr_counts"].astype(np.int64))
+    n = len(golden["gr_r4"])
+    L = golden["gr_box"][1] - golden["gr_box"][0]
+    g = po.gr_normalise(counts, n, float(L) ** 3, rstep)
+    assert g[0] == 0 and g.max() > 1.5  # the perturbed lattice's first shell
