@@ -120,6 +120,7 @@ void free_cells(Engine &e) {
   dfree(e, e.d_items);
   dfree(e, e.d_item0);
   dfree(e, e.fpartials);
+  dfree(e, e.fqueue);
   e.cells_ready = false;
 }
 
@@ -481,7 +482,8 @@ int engine_setup_cells(Engine &e) {
             dalloc(e, &e.colxy, xy_all.size()) == cudaSuccess &&
             dalloc(e, &e.d_sys, e.nsys) == cudaSuccess && dalloc(e, &e.d_items, items.size()) == cudaSuccess &&
             dalloc(e, &e.d_item0, e.nsys + 1) == cudaSuccess &&
-            dalloc(e, &e.fpartials, (size_t)4 * items.size()) == cudaSuccess;
+            dalloc(e, &e.fpartials, (size_t)4 * items.size()) == cudaSuccess &&
+            dalloc(e, &e.fqueue, 1) == cudaSuccess;
   if (!ok) {
     free_cells(e);
     return fail(e, PB_ERR_OOM, "cell list allocation failed");
@@ -577,6 +579,7 @@ ForceBufs engine_fbufs(Engine &e) {
   b.cap = (int)e.cap_max;
   b.F = e.F[e.cur];
   b.partials = e.fpartials;
+  b.queue = e.fqueue;
   b.status = e.status;
   b.steps_left = e.steps_left;
   return b;

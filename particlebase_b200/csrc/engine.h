@@ -73,6 +73,7 @@ struct Engine {
   uint32_t nitems = 0;
   std::vector<uint32_t> item0, cell0;
   double *fpartials = nullptr;
+  uint32_t *fqueue = nullptr;  // the force kernel's item counter
   uint32_t cap_max = 0;
   bool energy_valid = false;
 

@@ -871,6 +871,7 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
   __shared__ uint64_t full[2], empty[2], landed[2];
   __shared__ double cle[2][kWinCap][4];
   __shared__ int abort_flag, wait_ok;
+  __shared__ uint32_t next_item;
 
   const uint32_t slots = padded_slots((uint32_t)b.cap);
   const uint32_t pbytes = plane_bytes(slots, NT), wbytes = warp_bytes(slots);
@@ -914,17 +915,29 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
       producer_sync<kProd>();
       return ok;
     };
+    // Items are claimed from a global counter, so that a CTA that runs
+    // faster than the other CTA on its SM takes more of them (the result of an
+    // item does not depend on which CTA computes it).
     uint32_t lphase0 = 0u, lphase1 = 0u, running = 0;
     uint32_t n = 0;
     for (;; ++n) {
-      const uint32_t item = blockIdx.x + n * gridDim.x;
-      if (item >= b.nitems) break;
+      if (threadIdx.x == 0) next_item = atomicAdd(b.queue, 1u);
       const int bf = n & 1;
       if (n >= 2) {
         // the consumers are done with item n - 2 in this buffer
         if (!wait_empty(bf, ((n >> 1) - 1) & 1u)) return;
         if (ENERGY && threadIdx.x == 0) write_partials(b, desc[bf], cle[bf]);
-        producer_sync<kProd>();
+      }
+      producer_sync<kProd>();
+      const uint32_t item = next_item;
+      producer_sync<kProd>();
+      if (item >= b.nitems) {
+        // no item left: an end marker in this buffer stops the consumers
+        if (threadIdx.x == 0) {
+          desc[bf].item = kNone;
+          mbar_arrive(&full[bf]);
+        }
+        break;
       }
       const bool ok = produce_item<NT, MODE, kProd, kCons>(
           b, item, desc[bf], sc, planes(bf), &landed[bf], bf ? lphase1 : lphase0, running);
@@ -934,8 +947,9 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
       }
       if (threadIdx.x == 0) mbar_arrive(&full[bf]);
     }
-    // the last two items: wait for the consumers, then their energy partials
-    for (uint32_t m = n >= 2 ? n - 2 : 0; m < n; ++m) {
+    // the last item: wait for the consumers, then its energy partials
+    if (n >= 1) {
+      const uint32_t m = n - 1;
       const int bf = m & 1;
       if (!wait_empty(bf, (m >> 1) & 1u)) return;
       if (ENERGY && threadIdx.x == 0) write_partials(b, desc[bf], cle[bf]);
@@ -949,8 +963,6 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
       reinterpret_cast<uint16_t *>(smem_raw + 2 * (size_t)pbytes + (size_t)cw * wbytes);
   uint16_t *tb = mylist + 32 * kListLen;
   for (uint32_t n = 0;; ++n) {
-    const uint32_t item = blockIdx.x + n * gridDim.x;
-    if (item >= b.nitems) break;
     const int bf = n & 1;
     bool ok = lane != 0 || mbar_wait_or_abort(&full[bf], (n >> 1) & 1u, abort_v);
     ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -959,6 +971,7 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
       return;
     }
     const ItemDesc<NT> &d = desc[bf];
+    if (d.item == kNone) break;  // end marker
     const Planes pbuf = planes(bf);
     if (!d.skip) {
       if (!d.overflow) {
@@ -1012,6 +1025,8 @@ cudaError_t launch_w(const ForceBufs &b, cudaStream_t s) {
   // persistent grid: every resident CTA slot, at most one CTA per item
   const long slots = (long)resident_ctas(kern, (P + C) * 32, smem) * sm_count();
   const unsigned grid = (unsigned)std::min<long>(slots, (long)b.nitems);
+  e = cudaMemsetAsync(b.queue, 0, sizeof(uint32_t), s);
+  if (e != cudaSuccess) return e;
   kern<<<grid, (P + C) * 32, smem, s>>>(b);
   return cudaGetLastError();
 }

@@ -84,10 +84,11 @@ struct ForceBufs {
   uint32_t nitems;
   int cap;                   // shared-memory capacity of the launch (max over systems)
   float4 *F;                 // force output, particle order
-  double *partials;          // per-CTA energy partials (4 doubles per CTA)
+  double *partials;          // per-item energy partials (4 doubles per item)
   uint32_t *status;
   const uint32_t *steps_left;  // per system; 0 = finished, skipped (nullptr: all run)
   float sc_rc, sc_f0;          // soft-core force law: range and strength
+  uint32_t *queue;           // next unclaimed item (zeroed by the launch)
 };
 
 // Verlet neighbour list of one system: row s holds the build-time sorted
