@@ -716,15 +716,15 @@ __device__ __forceinline__ void consume_cluster(const ForceBufs &b, const ItemDe
   // entries at lbase + 64 k (entry k of lane `lane`)
   const uint32_t xa = smem_u32(X), ya = smem_u32(Y), za = smem_u32(Z);
   const uint32_t lbase = smem_u32(mylist) + 2u * (uint32_t)lane;
-  uint32_t o = 0;  // byte offset of this lane's next list entry
+  uint32_t oa = lbase;  // shared-memory address of this lane's next list entry
   // lane q tests quads u = q, q + 4, ... of the flat sequence, 4 per chunk; the
   // table pads the last chunk with the quad of far atoms
   for (uint32_t u0 = 0; u0 < Q; u0 += kChunk) {
-    const uint32_t cnt = o >> 6;
+    const uint32_t cnt = (oa - lbase) >> 6;
     if (__reduce_max_sync(0xffffffffu, cnt) > (uint32_t)(kListLen - kChunk)) {
       flush(cnt);
       __syncwarp();
-      o = 0;
+      oa = lbase;
     }
     const uint2 qq = *reinterpret_cast<const uint2 *>(tb + u0 + 4 * q);
     const uint32_t quads[4] = {qq.x & 0xffffu, qq.x >> 16, qq.y & 0xffffu, qq.y >> 16};
@@ -747,17 +747,17 @@ __device__ __forceinline__ void consume_cluster(const ForceBufs &b, const ItemDe
       // the stores are in bounds whether or not they are kept: the check above
       // leaves room for every candidate of this chunk
       const uint32_t s = quad * 4u;
-      sts_u16(lbase + o, s);
-      o += da.x < 0.0f ? 64u : 0u;
-      sts_u16(lbase + o, s + 1u);
-      o += da.y < 0.0f ? 64u : 0u;
-      sts_u16(lbase + o, s + 2u);
-      o += db.x < 0.0f ? 64u : 0u;
-      sts_u16(lbase + o, s + 3u);
-      o += db.y < 0.0f ? 64u : 0u;
+      sts_u16(oa, s);
+      oa += da.x < 0.0f ? 64u : 0u;
+      sts_u16(oa, s + 1u);
+      oa += da.y < 0.0f ? 64u : 0u;
+      sts_u16(oa, s + 2u);
+      oa += db.x < 0.0f ? 64u : 0u;
+      sts_u16(oa, s + 3u);
+      oa += db.y < 0.0f ? 64u : 0u;
     }
   }
-  flush(o >> 6);
+  flush((oa - lbase) >> 6);
   __syncwarp();
   float fx, fy, fz;
   Acc e0 = 0, e1 = 0, e2 = 0;
