@@ -144,18 +144,37 @@ __global__ void __launch_bounds__(kIntThreads) k_vv(IntegrateArgs a) {
   }
 }
 
-// A for atom i (FP64), identical arithmetic in both Gaussian passes.
-__device__ __forceinline__ void gauss_A(const IntegrateArgs &a, const SysInt &S, uint32_t i,
-                                        double xi_old, double A[3], float4 &F) {
-  const float h = (S.dt * 0.5f) * a.minv[i];
-  F = a.F[i];
-  const float4 Fo = a.Fold[i];
-  double v0[3];
-  load_v(a, S, i, v0);
-  const double hx = (double)S.dt * 0.5 * xi_old;
-  A[0] = v0[0] + (double)(F.x + Fo.x) * h - v0[0] * hx;
-  A[1] = v0[1] + (double)(F.y + Fo.y) * h - v0[1] * hx;
-  A[2] = v0[2] + (double)(F.z + Fo.z) * h - v0[2] * hx;
+// Per-atom inputs of the Gaussian passes, read through the read-only data
+// path.  A thread's atoms (kIntAtoms / kIntThreads, strided) are taken
+// kIntGroup at a time, the loads of a group issued before its arithmetic;
+// one atom at a time keeps the register count, and so the number of resident
+// threads, highest, which measured fastest.
+constexpr int kIntPer = kIntAtoms / kIntThreads;
+constexpr int kIntGroup = 1;
+
+struct GaussIn {
+  float4 F, Fo;
+  double v[3];
+  float minv, mass;
+};
+
+__device__ __forceinline__ void gauss_load(const IntegrateArgs &a, const SysInt &S, uint32_t i,
+                                           GaussIn &g) {
+  g.minv = __ldg(a.minv + i);
+  g.mass = __ldg(a.mass + i);
+  g.F = __ldg(a.F + i);
+  g.Fo = __ldg(a.Fold + i);
+  load_v(a, S, i, g.v);
+}
+
+// A for one atom (FP64), identical arithmetic in both Gaussian passes:
+// A = v + (F + Fold) dt/2m - v xi(t-dt) dt/2.
+__device__ __forceinline__ void gauss_A(const SysInt &S, const GaussIn &g, double hx,
+                                        double A[3]) {
+  const float h = (S.dt * 0.5f) * g.minv;
+  A[0] = g.v[0] + (double)(g.F.x + g.Fo.x) * h - g.v[0] * hx;
+  A[1] = g.v[1] + (double)(g.F.y + g.Fo.y) * h - g.v[1] * hx;
+  A[2] = g.v[2] + (double)(g.F.z + g.Fo.z) * h - g.v[2] * hx;
 }
 
 __global__ void __launch_bounds__(kIntThreads) k_gauss_a(IntegrateArgs a) {
@@ -165,14 +184,26 @@ __global__ void __launch_bounds__(kIntThreads) k_gauss_a(IntegrateArgs a) {
   const SysInt &S = a.sys[m.sys];
   DevScalars &sc = a.sc[m.sys];
   const double xi_old = sc.xi_old;
+  const double hx = (double)S.dt * 0.5 * xi_old;
   double s[2] = {0, 0};
-  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
-    const uint32_t i = m.i0 + t;
-    double A[3];
-    float4 F;
-    gauss_A(a, S, i, xi_old, A, F);
-    s[0] += (double)F.x * A[0] + (double)F.y * A[1] + (double)F.z * A[2];
-    s[1] += (double)a.mass[i] * (A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+#pragma unroll
+  for (int j0 = 0; j0 < kIntPer; j0 += kIntGroup) {
+    GaussIn g[kIntGroup];
+#pragma unroll
+    for (int j = 0; j < kIntGroup; ++j) {
+      const uint32_t t = threadIdx.x + (j0 + j) * kIntThreads;
+      if (t < m.n) gauss_load(a, S, m.i0 + t, g[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < kIntGroup; ++j) {
+      const uint32_t t = threadIdx.x + (j0 + j) * kIntThreads;
+      if (t < m.n) {
+        double A[3];
+        gauss_A(S, g[j], hx, A);
+        s[0] += (double)g[j].F.x * A[0] + (double)g[j].F.y * A[1] + (double)g[j].F.z * A[2];
+        s[1] += (double)g[j].mass * (A[0] * A[0] + A[1] * A[1] + A[2] * A[2]);
+      }
+    }
   }
   double tot[2];
   block_sum<2>(s, red);
@@ -198,30 +229,48 @@ __global__ void __launch_bounds__(kIntThreads) k_gauss_b(IntegrateArgs a) {
   DevScalars &sc = a.sc[m.sys];
   const double xi_old = sc.xi_old;
   const double xi = sc.xi_new;
+  const double hx = (double)S.dt * 0.5 * xi_old;
+  const double dt = S.dt;
+  const double inv = (xi_old == 0.0) ? 1.0 : 1.0 / (1.0 + xi * 0.5 * dt);
+  const double cv = dt - xi * 0.5 * dt * dt;
   double mv2 = 0;
-  for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
-    const uint32_t i = m.i0 + t;
-    double A[3];
-    float4 F;
-    gauss_A(a, S, i, xi_old, A, F);
-    const double dt = S.dt;
-    const double inv = (xi_old == 0.0) ? 1.0 : 1.0 / (1.0 + xi * 0.5 * dt);
-    const double v[3] = {A[0] * inv, A[1] * inv, A[2] * inv};
-    const double cv = dt - xi * 0.5 * dt * dt;
-    const double cf = 0.5 * dt * dt * (double)a.minv[i];
-    float4 p = a.r[i];
-    p.x = (float)((double)p.x + v[0] * cv + (double)F.x * cf);
-    p.y = (float)((double)p.y + v[1] * cv + (double)F.y * cf);
-    p.z = (float)((double)p.z + v[2] * cv + (double)F.z * cf);
-    if (a.wrap) wrap3(S, p);
-    a.r[i] = p;
-    if (a.vd) {
-      store_vd(a, S, i, v);
-      mv2 += (double)a.mass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-    } else {
-      const float4 vf = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
-      a.v[i] = vf;
-      mv2 += (double)a.mass[i] * ((double)vf.x * vf.x + (double)vf.y * vf.y + (double)vf.z * vf.z);
+#pragma unroll
+  for (int j0 = 0; j0 < kIntPer; j0 += kIntGroup) {
+    GaussIn g[kIntGroup];
+    float4 p[kIntGroup];
+#pragma unroll
+    for (int j = 0; j < kIntGroup; ++j) {
+      const uint32_t t = threadIdx.x + (j0 + j) * kIntThreads;
+      if (t < m.n) {
+        gauss_load(a, S, m.i0 + t, g[j]);
+        p[j] = a.r[m.i0 + t];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kIntGroup; ++j) {
+      const uint32_t t = threadIdx.x + (j0 + j) * kIntThreads;
+      if (t < m.n) {
+        const uint32_t i = m.i0 + t;
+        double A[3];
+        gauss_A(S, g[j], hx, A);
+        const double v[3] = {A[0] * inv, A[1] * inv, A[2] * inv};
+        const double cf = 0.5 * dt * dt * (double)g[j].minv;
+        float4 q = p[j];
+        q.x = (float)((double)q.x + v[0] * cv + (double)g[j].F.x * cf);
+        q.y = (float)((double)q.y + v[1] * cv + (double)g[j].F.y * cf);
+        q.z = (float)((double)q.z + v[2] * cv + (double)g[j].F.z * cf);
+        if (a.wrap) wrap3(S, q);
+        a.r[i] = q;
+        if (a.vd) {
+          store_vd(a, S, i, v);
+          mv2 += (double)g[j].mass * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        } else {
+          const float4 vf = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
+          a.v[i] = vf;
+          mv2 += (double)g[j].mass *
+                 ((double)vf.x * vf.x + (double)vf.y * vf.y + (double)vf.z * vf.z);
+        }
+      }
     }
   }
   double s[1] = {mv2}, tot[1];
