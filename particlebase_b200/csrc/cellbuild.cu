@@ -30,6 +30,7 @@ __device__ __forceinline__ uint32_t system_of(const CellBufs &b, uint32_t i) {
 }
 
 __global__ void __launch_bounds__(256) k_bin(CellBufs b) {
+  pdl_enter();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= b.N) return;
   const SysDesc &S = b.sys[system_of(b, i)];
@@ -46,6 +47,7 @@ __global__ void __launch_bounds__(256) k_bin(CellBufs b) {
 // Tile-local exclusive scan of kScanTile counts; writes the tile total and
 // zeroes the counts for the next build.
 __global__ void __launch_bounds__(1024) k_scan_tiles(CellBufs b) {
+  pdl_enter();
   __shared__ uint32_t warp_tot[32];
   const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * 4;
   uint32_t c[4];
@@ -90,6 +92,7 @@ __global__ void __launch_bounds__(1024) k_scan_tiles(CellBufs b) {
 
 // Exclusive scan of the tile totals (single block; up to 1024 * 32 tiles).
 __global__ void __launch_bounds__(1024) k_scan_top(CellBufs b, uint32_t ntiles) {
+  pdl_enter();
   __shared__ uint32_t warp_tot[32];
   __shared__ uint32_t carry;
   if (threadIdx.x == 0) carry = 0;
@@ -127,11 +130,13 @@ __global__ void __launch_bounds__(1024) k_scan_top(CellBufs b, uint32_t ntiles) 
 }
 
 __global__ void __launch_bounds__(256) k_scan_add(CellBufs b) {
+  pdl_enter();
   const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx < b.ncells) b.start[idx] += b.tilesum[idx / kScanTile];
 }
 
 __global__ void __launch_bounds__(256) k_scatter(CellBufs b) {
+  pdl_enter();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= b.N) return;
   b.pid_tmp[b.start[b.key[i]] + b.within[i]] = i;
@@ -198,6 +203,7 @@ __device__ void canon_large(const CellBufs &b, uint32_t s0, uint32_t n, int lane
 // half-warp orders one of them; otherwise the whole warp orders one, then the
 // other.
 __global__ void __launch_bounds__(256) k_canon(CellBufs b) {
+  pdl_enter();
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const uint32_t c0 = 2 * warp;
@@ -225,15 +231,17 @@ __global__ void __launch_bounds__(256) k_canon(CellBufs b) {
 cudaError_t launch_cell_build(const CellBufs &b, cudaStream_t s) {
   if (b.N == 0) return cudaSuccess;
   const uint32_t nb = (b.N + 255) / 256;
-  k_bin<<<nb, 256, 0, s>>>(b);
+  cudaError_t e = launch_pdl(k_bin, dim3(nb), dim3(256), 0, s, b);
   const uint32_t ntiles = (b.ncells + kScanTile - 1) / kScanTile;
-  k_scan_tiles<<<ntiles, 1024, 0, s>>>(b);
-  k_scan_top<<<1, 1024, 0, s>>>(b, ntiles);
-  k_scan_add<<<(b.ncells + 255) / 256, 256, 0, s>>>(b);
-  k_scatter<<<nb, 256, 0, s>>>(b);
+  if (e == cudaSuccess) e = launch_pdl(k_scan_tiles, dim3(ntiles), dim3(1024), 0, s, b);
+  if (e == cudaSuccess) e = launch_pdl(k_scan_top, dim3(1), dim3(1024), 0, s, b, ntiles);
+  if (e == cudaSuccess)
+    e = launch_pdl(k_scan_add, dim3((b.ncells + 255) / 256), dim3(256), 0, s, b);
+  if (e == cudaSuccess) e = launch_pdl(k_scatter, dim3(nb), dim3(256), 0, s, b);
   const uint64_t canon_threads = (uint64_t)((b.ncells + 1) / 2) * 32;
-  k_canon<<<(uint32_t)((canon_threads + 255) / 256), 256, 0, s>>>(b);
-  return cudaGetLastError();
+  if (e == cudaSuccess)
+    e = launch_pdl(k_canon, dim3((uint32_t)((canon_threads + 255) / 256)), dim3(256), 0, s, b);
+  return e;
 }
 
 }  // namespace pb

@@ -41,6 +41,37 @@ struct LJTable {
   float ushift[kMaxTypes * kMaxTypes];  // U(rc), for the shifted energy
 };
 
+// ---- programmatic dependent launch -------------------------------------------
+// The kernels of a step are launched with programmatic stream serialisation,
+// so that a kernel's CTAs are scheduled while its predecessor drains.  Every
+// such kernel calls pdl_enter() before anything else: it waits until the
+// predecessor has finished and its memory is visible (the same ordering as a
+// plain launch), then lets its own successor be scheduled.
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Launch `k` with programmatic stream serialisation; the kernel must begin
+// with pdl_enter().
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, args...);
+}
+#endif
+
 // ---- small device helpers ---------------------------------------------------
 #ifdef __CUDACC__
 

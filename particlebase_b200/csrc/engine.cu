@@ -483,12 +483,13 @@ int engine_setup_cells(Engine &e) {
             dalloc(e, &e.d_sys, e.nsys) == cudaSuccess && dalloc(e, &e.d_items, items.size()) == cudaSuccess &&
             dalloc(e, &e.d_item0, e.nsys + 1) == cudaSuccess &&
             dalloc(e, &e.fpartials, (size_t)4 * items.size()) == cudaSuccess &&
-            dalloc(e, &e.fqueue, 1) == cudaSuccess;
+            dalloc(e, &e.fqueue, 2) == cudaSuccess;
   if (!ok) {
     free_cells(e);
     return fail(e, PB_ERR_OOM, "cell list allocation failed");
   }
   E_CUDA(cudaMemsetAsync(e.count, 0, sizeof(uint32_t) * C, e.stream));
+  E_CUDA(cudaMemsetAsync(e.fqueue, 0, sizeof(uint32_t) * 2, e.stream));
   E_CUDA(cudaMemcpyAsync(e.colrank, rank_all.data(), 4 * rank_all.size(), cudaMemcpyHostToDevice,
                          e.stream));
   E_CUDA(cudaMemcpyAsync(e.colxy, xy_all.data(), 4 * xy_all.size(), cudaMemcpyHostToDevice,

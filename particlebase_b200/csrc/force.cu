@@ -865,6 +865,7 @@ __device__ void consume_task_global(const ForceBufs &b, const ItemDesc<NT> &d, u
 template <int NT, bool ENERGY, typename Acc, int kProd, int kCons, int MODE>
 __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 1 : 2)
     k_force(ForceBufs b) {
+  pdl_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ ItemDesc<NT> desc[2];
   __shared__ Scratch sc;
@@ -915,9 +916,20 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
       producer_sync<kProd>();
       return ok;
     };
-    // Items are claimed from a global counter, so that a CTA that runs
-    // faster than the other CTA on its SM takes more of them (the result of an
-    // item does not depend on which CTA computes it).
+    // Items are claimed from a global counter (queue[0]), so that a CTA that
+    // runs faster than the other CTA on its SM takes more of them (the result
+    // of an item does not depend on which CTA computes it).  A CTA that will
+    // claim no more counts itself in queue[1]; the last one resets both for
+    // the next launch.
+    auto done_claiming = [&]() {
+      if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(b.queue + 1, 1u) == gridDim.x - 1) {
+          atomicExch(b.queue, 0u);
+          atomicExch(b.queue + 1, 0u);
+        }
+      }
+    };
     uint32_t lphase0 = 0u, lphase1 = 0u, running = 0;
     uint32_t n = 0;
     for (;; ++n) {
@@ -925,7 +937,10 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
       const int bf = n & 1;
       if (n >= 2) {
         // the consumers are done with item n - 2 in this buffer
-        if (!wait_empty(bf, ((n >> 1) - 1) & 1u)) return;
+        if (!wait_empty(bf, ((n >> 1) - 1) & 1u)) {
+          done_claiming();
+          return;
+        }
         if (ENERGY && threadIdx.x == 0) write_partials(b, desc[bf], cle[bf]);
       }
       producer_sync<kProd>();
@@ -933,6 +948,7 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
       producer_sync<kProd>();
       if (item >= b.nitems) {
         // no item left: an end marker in this buffer stops the consumers
+        done_claiming();
         if (threadIdx.x == 0) {
           desc[bf].item = kNone;
           mbar_arrive(&full[bf]);
@@ -942,6 +958,7 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
       const bool ok = produce_item<NT, MODE, kProd, kCons>(
           b, item, desc[bf], sc, planes(bf), &landed[bf], bf ? lphase1 : lphase0, running);
       if (!ok) {
+        done_claiming();
         if (threadIdx.x == 0) abort_flag = 1;
         return;
       }
@@ -1025,10 +1042,7 @@ cudaError_t launch_w(const ForceBufs &b, cudaStream_t s) {
   // persistent grid: every resident CTA slot, at most one CTA per item
   const long slots = (long)resident_ctas(kern, (P + C) * 32, smem) * sm_count();
   const unsigned grid = (unsigned)std::min<long>(slots, (long)b.nitems);
-  e = cudaMemsetAsync(b.queue, 0, sizeof(uint32_t), s);
-  if (e != cudaSuccess) return e;
-  kern<<<grid, (P + C) * 32, smem, s>>>(b);
-  return cudaGetLastError();
+  return launch_pdl(kern, dim3(grid), dim3((P + C) * 32), smem, s, b);
 }
 
 // Launch shapes (producer warps, consumer warps): the default, and a small one.

@@ -109,6 +109,7 @@ __device__ __forceinline__ void load_v(const IntegrateArgs &a, const SysInt &S, 
 }
 
 __global__ void __launch_bounds__(kIntThreads) k_vv(IntegrateArgs a) {
+  pdl_enter();
   __shared__ double red[32];
   const BlockMap m = a.map[blockIdx.x];
   if (finished(a, m.sys)) return;
@@ -178,6 +179,7 @@ __device__ __forceinline__ void gauss_A(const SysInt &S, const GaussIn &g, doubl
 }
 
 __global__ void __launch_bounds__(kIntThreads) k_gauss_a(IntegrateArgs a) {
+  pdl_enter();
   __shared__ double red[2 * 32];
   const BlockMap m = a.map[blockIdx.x];
   if (finished(a, m.sys)) return;
@@ -222,6 +224,7 @@ __global__ void __launch_bounds__(kIntThreads) k_gauss_a(IntegrateArgs a) {
 }
 
 __global__ void __launch_bounds__(kIntThreads) k_gauss_b(IntegrateArgs a) {
+  pdl_enter();
   __shared__ double red[32];
   const BlockMap m = a.map[blockIdx.x];
   if (finished(a, m.sys)) return;
@@ -556,7 +559,10 @@ void make_block_map(const uint32_t *natoms, uint32_t nsys, BlockMap *map, uint32
     return cudaGetLastError();                                                  \
   } while (0)
 
-cudaError_t launch_vv(const IntegrateArgs &a, cudaStream_t s) { PB_LAUNCH(k_vv, a); }
+cudaError_t launch_vv(const IntegrateArgs &a, cudaStream_t s) {
+  if (!a.nblocks) return cudaSuccess;
+  return launch_pdl(k_vv, dim3(a.nblocks), dim3(kIntThreads), 0, s, a);
+}
 cudaError_t launch_wrap(const IntegrateArgs &a, cudaStream_t s) { PB_LAUNCH(k_wrap, a); }
 cudaError_t launch_mv2(const IntegrateArgs &a, cudaStream_t s) { PB_LAUNCH(k_mv2, a); }
 cudaError_t launch_fv(const IntegrateArgs &a, cudaStream_t s) { PB_LAUNCH(k_fv, a); }
@@ -566,9 +572,9 @@ cudaError_t launch_scale(const IntegrateArgs &a, const double *f, cudaStream_t s
 
 cudaError_t launch_gauss(const IntegrateArgs &a, cudaStream_t s) {
   if (!a.nblocks) return cudaSuccess;
-  k_gauss_a<<<a.nblocks, kIntThreads, 0, s>>>(a);
-  k_gauss_b<<<a.nblocks, kIntThreads, 0, s>>>(a);
-  return cudaGetLastError();
+  cudaError_t e = launch_pdl(k_gauss_a, dim3(a.nblocks), dim3(kIntThreads), 0, s, a);
+  if (e == cudaSuccess) e = launch_pdl(k_gauss_b, dim3(a.nblocks), dim3(kIntThreads), 0, s, a);
+  return e;
 }
 
 cudaError_t launch_adjust(const IntegrateArgs &a, const double *v1, cudaStream_t s) {

@@ -88,7 +88,8 @@ struct ForceBufs {
   uint32_t *status;
   const uint32_t *steps_left;  // per system; 0 = finished, skipped (nullptr: all run)
   float sc_rc, sc_f0;          // soft-core force law: range and strength
-  uint32_t *queue;           // next unclaimed item (zeroed by the launch)
+  uint32_t *queue;           // [0] next unclaimed item, [1] CTAs done claiming; zero
+                             // between launches (the last CTA resets them)
 };
 
 // Verlet neighbour list of one system: row s holds the build-time sorted
