@@ -1,4 +1,6 @@
 #include "engine.h"
+#include <atomic>
+#include <thread>
 
 #include <algorithm>
 #include <cmath>
@@ -360,44 +362,82 @@ void engine_set_dt(Engine &e, float dt) {
   if (changed) engine_upload_sysint(e);
 }
 
+// Host conversion of imported atoms runs on several threads over fixed
+// chunks; per-chunk mass sums are added in chunk order, so the mean mass does
+// not depend on the number of threads.
+constexpr uint32_t kImportChunk = 1u << 16;
+
+template <typename F>
+void for_chunks(uint32_t n, F &&body) {
+  const uint32_t nchunks = (n + kImportChunk - 1) / kImportChunk;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned nth = std::min<unsigned>(std::min(hw, 16u), nchunks);
+  std::atomic<uint32_t> next{0};
+  auto run = [&]() {
+    for (uint32_t c; (c = next.fetch_add(1)) < nchunks;)
+      body(c, c * kImportChunk, std::min(n, (c + 1) * kImportChunk));
+  };
+  std::vector<std::thread> th;
+  for (unsigned k = 1; k < nth; ++k) th.emplace_back(run);
+  run();
+  for (auto &t : th) t.join();
+}
+
 int engine_import(Engine &e, uint32_t sys, const double *r3, const double *v3, const double *mass,
                   const uint32_t *type) {
   if (sys >= e.nsys || !r3) return fail(e, PB_ERR_ARG, "bad system or positions");
+  e.mv2_fresh = false;
   const uint32_t n = e.sp[sys].n, a0 = e.atom0[sys];
-  std::vector<float4> r4(n), v4(n, make_float4(0, 0, 0, 0));
-  std::vector<float> minv(n, 1.f), m(n, 1.f);
-  std::vector<uint16_t> t(n, 0);
-  double msum = 0;
-  for (uint32_t i = 0; i < n; ++i) {
-    r4[i] = make_float4((float)r3[3 * i], (float)r3[3 * i + 1], (float)r3[3 * i + 2], 0.f);
-    if (v3) v4[i] = make_float4((float)v3[3 * i], (float)v3[3 * i + 1], (float)v3[3 * i + 2], 0.f);
-    const double mi = mass ? mass[i] : 1.0;
-    if (!(mi > 0)) return fail(e, PB_ERR_ARG, "mass must be positive");
-    minv[i] = (float)(1.0 / mi);  // cudaParticleBase::import: TMP[i] = 1.0 / m
-    m[i] = 1.0f / minv[i];        // cudaParticleMD::setM: m = 1 / minv
-    msum += mi;
-    if (type) {
-      if (type[i] >= (uint32_t)kMaxTypes) return fail(e, PB_ERR_ARG, "type id >= 8");
-      t[i] = (uint16_t)type[i];
+  if (n == 0) return PB_OK;
+  std::unique_ptr<float4[]> r4(new float4[n]), v4(e.vd ? nullptr : new float4[n]);
+  std::unique_ptr<float[]> minv(new float[n]), m(new float[n]);
+  std::unique_ptr<uint16_t[]> t(new uint16_t[n]);
+  std::unique_ptr<double[]> vd(e.vd ? new double[(size_t)3 * n] : nullptr);
+  const uint32_t nchunks = (n + kImportChunk - 1) / kImportChunk;
+  std::vector<double> msum(nchunks, 0.0);
+  std::vector<int> bad(nchunks, 0);  // 1: mass, 2: type
+  for_chunks(n, [&](uint32_t c, uint32_t i0, uint32_t i1) {
+    double ms = 0;
+    for (uint32_t i = i0; i < i1; ++i) {
+      r4[i] = make_float4((float)r3[3 * i], (float)r3[3 * i + 1], (float)r3[3 * i + 2], 0.f);
+      if (v4)
+        v4[i] = v3 ? make_float4((float)v3[3 * i], (float)v3[3 * i + 1], (float)v3[3 * i + 2], 0.f)
+                   : make_float4(0.f, 0.f, 0.f, 0.f);
+      if (vd)
+        for (int k = 0; k < 3; ++k) vd[(size_t)k * n + i] = v3 ? v3[3 * i + k] : 0.0;
+      const double mi = mass ? mass[i] : 1.0;
+      if (!(mi > 0)) bad[c] |= 1;
+      minv[i] = (float)(1.0 / mi);  // cudaParticleBase::import: TMP[i] = 1.0 / m
+      m[i] = 1.0f / minv[i];        // cudaParticleMD::setM: m = 1 / minv
+      ms += mi;
+      uint16_t ti = 0;
+      if (type) {
+        if (type[i] >= (uint32_t)kMaxTypes) bad[c] |= 2;
+        ti = (uint16_t)type[i];
+      }
+      t[i] = ti;
     }
+    msum[c] = ms;
+  });
+  double total = 0;
+  int flags = 0;
+  for (uint32_t c = 0; c < nchunks; ++c) {
+    total += msum[c];
+    flags |= bad[c];
   }
-  e.sp[sys].m0 = msum / n;
-  E_CUDA(cudaMemcpyAsync(e.r + a0, r4.data(), 16 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
-  E_CUDA(cudaMemcpyAsync(e.minv + a0, minv.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
-  E_CUDA(cudaMemcpyAsync(e.mass + a0, m.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
-  E_CUDA(cudaMemcpyAsync(e.type + a0, t.data(), 2 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
-  if (e.vd) {
-    std::vector<double> vd((size_t)3 * n, 0.0);
-    if (v3)
-      for (uint32_t i = 0; i < n; ++i)
-        for (int k = 0; k < 3; ++k) vd[(size_t)k * n + i] = v3[3 * i + k];
-    E_CUDA(cudaMemcpyAsync(e.vd + 3 * (size_t)a0, vd.data(), 24 * (size_t)n,
+  if (flags & 1) return fail(e, PB_ERR_ARG, "mass must be positive");
+  if (flags & 2) return fail(e, PB_ERR_ARG, "type id >= 8");
+  e.sp[sys].m0 = total / n;
+  E_CUDA(cudaMemcpyAsync(e.r + a0, r4.get(), 16 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
+  E_CUDA(cudaMemcpyAsync(e.minv + a0, minv.get(), 4 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
+  E_CUDA(cudaMemcpyAsync(e.mass + a0, m.get(), 4 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
+  E_CUDA(cudaMemcpyAsync(e.type + a0, t.get(), 2 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
+  if (e.vd)
+    E_CUDA(cudaMemcpyAsync(e.vd + 3 * (size_t)a0, vd.get(), 24 * (size_t)n,
                            cudaMemcpyHostToDevice, e.stream));
-    E_CUDA(cudaStreamSynchronize(e.stream));
-  } else {
-    E_CUDA(cudaMemcpyAsync(e.v + a0, v4.data(), 16 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
-    E_CUDA(cudaStreamSynchronize(e.stream));
-  }
+  else
+    E_CUDA(cudaMemcpyAsync(e.v + a0, v4.get(), 16 * (size_t)n, cudaMemcpyHostToDevice, e.stream));
+  E_CUDA(cudaStreamSynchronize(e.stream));
   return PB_OK;
 }
 
@@ -753,6 +793,9 @@ int engine_evolve(Engine &e, int mode, int wrap) {
   if (c != cudaSuccess) return cuda_fail(e, c, "time evolution");
   e.cur = 1 - e.cur;
   ++e.steps_done;
+  // k_vv and k_gauss_b end with sum m v^2 of the new velocities, added in the
+  // same order as k_mv2, so a temperature read needs no further kernel
+  e.mv2_fresh = true;
   return PB_OK;
 }
 
@@ -784,6 +827,7 @@ int engine_run(Engine &e, int mode, uint32_t steps) {
     cudaGraph_t g = nullptr;
     const int cur0 = e.cur, last0 = e.last;
     const uint64_t done0 = e.steps_done;
+    const bool fresh0 = e.mv2_fresh;
     E_CUDA(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
     int rc = PB_OK;
     for (int k = 0; k < n && !rc; ++k) rc = engine_step(e, mode);
@@ -791,6 +835,7 @@ int engine_run(Engine &e, int mode, uint32_t steps) {
     e.cur = cur0;  // the captured steps have not run yet
     e.last = last0;
     e.steps_done = done0;
+    e.mv2_fresh = fresh0;
     if (rc) {
       if (g) cudaGraphDestroy(g);
       return rc;
@@ -828,6 +873,7 @@ int engine_run(Engine &e, int mode, uint32_t steps) {
     e.last = e.cur;
     e.cur = 1 - e.cur;
   }
+  if (steps > 0) e.mv2_fresh = true;  // each step ends with sum m v^2
   e.energy_valid = false;
   return PB_OK;
 }
@@ -909,6 +955,7 @@ int engine_clear_force(Engine &e) {
 int engine_mv2(Engine &e) {
   cudaError_t c = launch_mv2(engine_iargs(e, 0), e.stream);
   if (c != cudaSuccess) return cuda_fail(e, c, "mv2");
+  e.mv2_fresh = true;
   return PB_OK;
 }
 
@@ -919,6 +966,7 @@ int engine_fv(Engine &e) {
 }
 
 int engine_scale(Engine &e, const double *factors) {
+  e.mv2_fresh = false;
   E_CUDA(cudaMemcpyAsync(e.d_fac, factors, sizeof(double) * e.nsys, cudaMemcpyHostToDevice,
                          e.stream));
   cudaError_t c = launch_scale(engine_iargs(e, 0), e.d_fac, e.stream);
@@ -928,6 +976,7 @@ int engine_scale(Engine &e, const double *factors) {
 }
 
 int engine_adjust(Engine &e, const double *v1) {
+  e.mv2_fresh = false;
   E_CUDA(cudaMemcpyAsync(e.d_fac, v1, sizeof(double) * e.nsys, cudaMemcpyHostToDevice, e.stream));
   cudaError_t c = launch_adjust(engine_iargs(e, 0), e.d_fac, e.stream);
   if (c != cudaSuccess) return cuda_fail(e, c, "adjust");
@@ -951,6 +1000,7 @@ int engine_force_softcore(Engine &e, float rc, float f0) {
 }
 
 int engine_euler(Engine &e, float dt) {
+  e.mv2_fresh = false;
   if (!e.v) return fail(e, PB_ERR_UNSUPPORTED, "the Euler step uses FP32 velocities");
   cudaError_t c = launch_euler(engine_iargs(e, 1), e.F[e.last], dt, e.stream);
   if (c != cudaSuccess) return cuda_fail(e, c, "Euler step");

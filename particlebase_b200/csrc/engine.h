@@ -76,6 +76,7 @@ struct Engine {
   uint32_t *fqueue = nullptr;  // the force kernel's item counter
   uint32_t cap_max = 0;
   bool energy_valid = false;
+  bool mv2_fresh = false;  // sc.mv2 holds sum m v^2 of the current velocities
 
   // Verlet neighbour list (single-system handles; see nlist.cu): while on,
   // force calls use the list and whole steps skip the cell-list build

@@ -299,8 +299,10 @@ int pb_md_reduce(pb_md *h, pb_md_sums *out) {
 
 int pb_md_temperature(pb_md *h, double *T) {
   if (!h || !T) return PB_ERR_ARG;
-  const int rc = engine_mv2(h->e);
-  if (rc) return rc;
+  if (!h->e.mv2_fresh) {  // otherwise the last step's sum is still current
+    const int rc = engine_mv2(h->e);
+    if (rc) return rc;
+  }
   double mv2 = 0;
   H_CUDA(cudaMemcpyAsync(&mv2, &h->e.sc[0].mv2, sizeof(double), cudaMemcpyDeviceToHost,
                          h->e.stream));
@@ -418,6 +420,7 @@ int pb_md_set(pb_md *h, int field, const void *host, size_t bytes) {
   const int rc = pb_md_field_bytes(h, field, &need);
   if (rc) return rc;
   if (bytes != need) return fail(h, PB_ERR_ARG, "size mismatch for field");
+  e.mv2_fresh = false;  // velocities or masses may change
   void *dst = nullptr;
   switch (field) {
     case PB_FIELD_R: dst = e.r; break;
