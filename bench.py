@@ -56,6 +56,12 @@ def dist_env():
     return ws, rank, local
 
 
+def replica_rate(ws: int, atoms: int, steps: int, seconds_max: float) -> float:
+    """Whole-job atom-steps/s of `ws` independent replicas of `atoms` atoms each
+    (one per rank, weak scaling), from the slowest rank's time."""
+    return ws * atoms * steps / seconds_max
+
+
 class Dist:
     """torch.distributed plumbing: barrier and max/sum over ranks."""
 
@@ -260,7 +266,7 @@ def run_ours(args, dist: Dist) -> dict:
     clocks = clk.summary()
     status = p.status()
     t_max = dist.reduce(t_ms, "max") / 1e3
-    value = dist.ws * s.n * steps / t_max
+    value = replica_rate(dist.ws, s.n, steps, t_max)
     warm_value = s.n * steps / (warm_ms / 1e3)
 
     # phase breakdown and the force kernel's roofline
@@ -297,7 +303,7 @@ def run_ours(args, dist: Dist) -> dict:
     r_final = q.getPosition()
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    e2e_value = dist.ws * s.n * e2e_steps / dist.reduce(e2e_s, "max")
+    e2e_value = replica_rate(dist.ws, s.n, e2e_steps, dist.reduce(e2e_s, "max"))
     h2d = s.n * (16 + 16 + 4 + 4 + 2)
     d2h = 8 * e2e_steps + r_final.nbytes
     q.close()
@@ -447,8 +453,8 @@ def run_batched(args, dist: Dist) -> dict:
     q.close()
     e2e_s = dist.reduce(e2e_s, "max")
 
-    v_batched = dist.ws * total * steps / (batched_ms / 1e3)
-    v_plain = dist.ws * total * steps / (plain_ms / 1e3)
+    v_batched = replica_rate(dist.ws, total, steps, batched_ms / 1e3)
+    v_plain = replica_rate(dist.ws, total, steps, plain_ms / 1e3)
     return {
         "metric": "batched-replica atom-steps/s (256 uneven LJ replicas)",
         "value": v_batched, "unit": UNIT, "ms_per_step": batched_ms / steps,
@@ -459,7 +465,7 @@ def run_batched(args, dist: Dist) -> dict:
         "atoms_min": int(natoms.min()), "atoms_max": int(natoms.max()),
         "tuning": {k: tune[k] for k in ("threads", "seg_scale", "cached")},
         "phase_ms": prof, "device_status": status,
-        "e2e": {"value": dist.ws * total * steps / e2e_s, "unit": UNIT,
+        "e2e": {"value": replica_rate(dist.ws, total, steps, e2e_s), "unit": UNIT,
                 "h2d_bytes_per_step": total * 42 / steps, "d2h_bytes_per_step": total * 16 / steps,
                 "includes": "batch creation from host arrays, all steps, final positions to host"},
         "config": {"workload": "lj_uneven_replicas_256_gauss", "dt": DT, "seed": 3 + dist.rank,
@@ -558,7 +564,7 @@ def run_kob_andersen(args, dist: Dist) -> dict:
     p.close()
     return {
         "metric": "LJ atom-steps/s, Kob-Andersen 8.4M atoms", "unit": UNIT,
-        "value": dist.ws * s.n * steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps,
+        "value": replica_rate(dist.ws, s.n, steps, ms / 1e3), "ms_per_step": ms / steps, "steps": steps,
         "atoms": s.n, "relax_s": relax_s, "temperature": T, "pe_per_atom": sums["pe"] / s.n,
         "phase_ms": prof, "ncand_per_atom": ps["ncand"] / s.n, "nin_per_atom": ps["nin"] / s.n,
         "flops_per_atom_step": (8 * ps["ncand"] + 14 * ps["nin"]) / s.n,
