@@ -44,14 +44,22 @@ __device__ __forceinline__ float round_image(float d, float L, float Linv) {
   return d - L * rintf(d * Linv);
 }
 
-__global__ void __launch_bounds__(kNlThreads) k_nlist_build(NlistBufs b) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= b.N) return;
+// Row s of the list, built by one thread; returns its length (entries beyond
+// the capacity are counted, not stored).  The three cells z - 1, z, z + 1 of a neighbour column
+// are consecutive in sorted order and sorted by z, so each column is one
+// range: a binary search finds its first atom inside the atom's z window,
+// and the scan stops at the first atom above it.  The window half-width
+// shrinks with the atom's distance in x and y from that column, a bound
+// taken with a margin of 10^-3 cell edges (cell membership is decided in
+// FP32).  The column's periodic image is applied as one shift.  A column
+// whose z cells wrap around the box (z = 0 or nz - 1) is scanned cell by
+// cell, with a shift per cell.  Candidates are visited in sorted order, so a
+// row lists its atoms in the same order as a scan of the 27 cells.
+__device__ uint32_t nlist_row(const NlistBufs &b, uint32_t s) {
   const SysDesc &S = b.sys[0];
   const Grid g = S.g;
   const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
   const float Lx = g.L[0], Ly = g.L[1], Lz = g.L[2];
-  const float iLx = 1.0f / Lx, iLy = 1.0f / Ly, iLz = 1.0f / Lz;
   const uint32_t i = b.pid[s];
   const float4 p = b.rs[s];
   const uint32_t kk = b.key[i] - S.cell0;
@@ -59,30 +67,73 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_build(NlistBufs b) {
   const int z = (int)(kk - rank * (uint32_t)nz);
   const uint32_t xy = b.colxy[S.col0 + rank];
   const int d0 = (int)(xy / (uint32_t)ny), d1 = (int)(xy % (uint32_t)ny);
+  // distances to the home cell's x and y faces, less the margin
+  const float mx = 1e-3f * g.len[0], my = 1e-3f * g.len[1];
+  const float xlo = g.lo[0] + (float)d0 * g.len[0], xhi = xlo + g.len[0];
+  const float ylo = g.lo[1] + (float)d1 * g.len[1], yhi = ylo + g.len[1];
+  const float ex_lo = fmaxf(p.x - xlo - mx, 0.f), ex_hi = fmaxf(xhi - p.x - mx, 0.f);
+  const float ey_lo = fmaxf(p.y - ylo - my, 0.f), ey_hi = fmaxf(yhi - p.y - my, 0.f);
+  const bool wraps = z == 0 || z == nz - 1;
   uint32_t n = 0;
+  auto take = [&](uint32_t t, float qx, float qy, float qz, float sx, float sy, float sz) {
+    const float dx = (qx + sx) - p.x, dy = (qy + sy) - p.y, dz = (qz + sz) - p.z;
+    if (t != s && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < b.rl2) {
+      if (n < b.cap) b.idx[(size_t)n * b.N + s] = t;
+      ++n;
+    }
+  };
   for (int a = -1; a <= 1; ++a) {
+    const float ex = a < 0 ? ex_lo : (a > 0 ? ex_hi : 0.f);
+    const float sx = d0 + a < 0 ? -Lx : (d0 + a >= nx ? Lx : 0.f);
     for (int c = -1; c <= 1; ++c) {
+      const float ey = c < 0 ? ey_lo : (c > 0 ? ey_hi : 0.f);
+      const float rem = b.rl2 - fmaf(ex, ex, ey * ey);
+      if (!(rem > 0.f)) continue;  // the whole column is out of range
+      const float sy = d1 + c < 0 ? -Ly : (d1 + c >= ny ? Ly : 0.f);
       const int c0 = (d0 + a + nx) % nx, c1 = (d1 + c + ny) % ny;
       const uint32_t rk = b.colrank[S.col0 + (uint32_t)(c0 * ny + c1)];
-      for (int e = -1; e <= 1; ++e) {
-        const uint32_t key2 = S.cell0 + rk * (uint32_t)nz + (uint32_t)((z + e + nz) % nz);
-        const uint32_t t0 = b.start[key2], t1 = b.start[key2 + 1];
-        // four candidates per pass, their loads issued together
-        for (uint32_t tb = t0; tb < t1; tb += 4) {
-          float4 q[4];
+      const uint32_t kb = S.cell0 + rk * (uint32_t)nz;
+      if (wraps) {
+        for (int e = -1; e <= 1; ++e) {
+          const int ze = z + e;
+          const float sz = ze < 0 ? -Lz : (ze >= nz ? Lz : 0.f);
+          const uint32_t key2 = kb + (uint32_t)((ze + nz) % nz);
+          const uint32_t t1 = b.start[key2 + 1];
+          for (uint32_t t0 = b.start[key2]; t0 < t1; t0 += 4) {
+            float4 q[4];  // four candidates per pass, their loads issued together
 #pragma unroll
-          for (int u = 0; u < 4; ++u) q[u] = b.rs[min(tb + u, t1 - 1)];
+            for (int u = 0; u < 4; ++u) q[u] = b.rs[min(t0 + u, t1 - 1)];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const uint32_t t = tb + u;
-            const float dx = round_image(q[u].x - p.x, Lx, iLx);
-            const float dy = round_image(q[u].y - p.y, Ly, iLy);
-            const float dz = round_image(q[u].z - p.z, Lz, iLz);
-            if (t < t1 && t != s && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < b.rl2) {
-              if (n < b.cap) b.idx[(size_t)n * b.N + s] = t;
-              ++n;
-            }
+            for (int u = 0; u < 4; ++u)
+              if (t0 + u < t1) take(t0 + u, q[u].x, q[u].y, q[u].z, sx, sy, sz);
           }
+        }
+        continue;
+      }
+      const float dzw = sqrtf(rem) * 1.0001f;
+      const float zlo = p.z - dzw, zhi = p.z + dzw;
+      uint32_t lo = b.start[kb + (uint32_t)(z - 1)];
+      uint32_t hi = b.start[kb + (uint32_t)(z + 2)];
+      // first atom with z >= zlo
+      uint32_t len = hi - lo;
+      while (len > 0) {
+        const uint32_t half = len >> 1;
+        if (__ldg(&b.rs[lo + half].z) < zlo) {
+          lo += half + 1;
+          len -= half + 1;
+        } else {
+          len = half;
+        }
+      }
+      bool past = false;
+      for (uint32_t t0 = lo; t0 < hi && !past; t0 += 4) {
+        float4 q[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) q[u] = b.rs[min(t0 + u, hi - 1)];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          past = past || t0 + u >= hi || q[u].z > zhi;
+          if (!past) take(t0 + u, q[u].x, q[u].y, q[u].z, sx, sy, 0.f);
         }
       }
     }
@@ -91,7 +142,16 @@ __global__ void __launch_bounds__(kNlThreads) k_nlist_build(NlistBufs b) {
   b.atom[s] = i;
   b.r0[s] = make_float4(p.x, p.y, p.z, 0.0f);
   if (n > b.cap) atomicOr(&b.status[0], kStatusNlistOverflow);
-  atomicMax(b.maxcnt, n);
+  return n;
+}
+
+__global__ void __launch_bounds__(kNlThreads) k_nlist_build(NlistBufs b) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  // the longest row goes to one counter: a maximum over the warp first, then
+  // one atomic per warp (an atomic per row on one address serialises)
+  const uint32_t n = s < b.N ? nlist_row(b, s) : 0u;
+  const uint32_t wmax = __reduce_max_sync(0xffffffffu, n);
+  if ((threadIdx.x & 31) == 0 && wmax > 0) atomicMax(b.maxcnt, wmax);
 }
 
 // Current positions in row order, so the pair loop gathers from build-time
