@@ -682,6 +682,9 @@ __device__ __forceinline__ void consume_cluster(const ForceBufs &b, const ItemDe
   const float xi = valid ? X[hs] : kNoAtom;
   const float yi = valid ? Y[hs] : kNoAtom;
   const float zi = valid ? Z[hs] : kNoAtom;
+  // the particle index of the force store, fetched now so that its latency
+  // passes during the pair loops
+  const uint32_t pi = valid && q == 0 ? __ldg(b.pid + d.home_g0 + h) : 0u;
   const int ti = NT == 1 ? 0 : (int)T[hs];
   // the warp's quad table: lanes cover (column, index) pairs, column = idx / M
   // by a multiply-high (exact while 9 M^2 < 2^32)
@@ -796,10 +799,7 @@ __device__ __forceinline__ void consume_cluster(const ForceBufs &b, const ItemDe
       e3 = acc.n;
     }
   }
-  if (valid && q == 0) {
-    const uint32_t gh = d.home_g0 + h;
-    b.F[b.pid[gh]] = make_float4(fx, fy, fz, 0.0f);
-  }
+  if (valid && q == 0) b.F[pi] = make_float4(fx, fy, fz, 0.0f);
   if (ENERGY) {
     ce[0] = warp_sum((double)e0);
     ce[1] = warp_sum((double)e1);
