@@ -153,7 +153,7 @@ int pb_batch_repack(const pb_batch *old, const int32_t *src, const uint32_t *nat
   }
   // all continuing systems' per-atom state in one launch
   GatherSrc *d_gs = nullptr;
-  if (cudaMallocAsync((void **)&d_gs, sizeof(GatherSrc) * nsys, e.stream) != cudaSuccess ||
+  if (engine_alloc_bytes(e, (void **)&d_gs, sizeof(GatherSrc) * nsys) != cudaSuccess ||
       cudaMemcpyAsync(d_gs, gs.data(), sizeof(GatherSrc) * nsys, cudaMemcpyHostToDevice,
                       e.stream) != cudaSuccess)
     return bail(PB_ERR_CUDA);
@@ -179,7 +179,7 @@ int pb_batch_repack(const pb_batch *old, const int32_t *src, const uint32_t *nat
   ga.mass = e.mass;
   ga.type = e.type;
   const cudaError_t gc = launch_gather_state(ga, e.stream);
-  cudaFreeAsync(d_gs, e.stream);
+  engine_free_bytes(e, d_gs);
   if (gc != cudaSuccess) return bail(PB_ERR_CUDA);
   if (cudaMemcpyAsync(e.sc, nsc.data(), sizeof(DevScalars) * nsys, cudaMemcpyHostToDevice,
                       e.stream) != cudaSuccess ||

@@ -71,6 +71,23 @@ void dfree(Engine &e, T *&p) {
   p = nullptr;
 }
 
+}  // namespace
+
+// Scratch of the batch and server paths comes from the same pool: memory from
+// CUDA's default pool (release threshold 0) made stream synchronisations
+// after a repack stall for hundreds of milliseconds.
+cudaError_t engine_alloc_bytes(Engine &e, void **p, size_t bytes) {
+  cudaMemPool_t pool = device_pool();
+  if (!pool) return cudaErrorMemoryAllocation;
+  return cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, e.stream);
+}
+
+void engine_free_bytes(Engine &e, void *p) {
+  if (p) cudaFreeAsync(p, e.stream);
+}
+
+namespace {
+
 // Column ranking and force work items depend only on the grid and the z-run
 // length; batches of many similar systems share them.
 struct PlanKey {

@@ -120,6 +120,9 @@ int engine_force(Engine &e, bool energy);
 int engine_evolve(Engine &e, int mode, int wrap);
 int engine_wrap(Engine &e);
 int engine_step(Engine &e, int mode);
+// Device scratch from the engine's pool, on its stream (stream-ordered).
+cudaError_t engine_alloc_bytes(Engine &e, void **p, size_t bytes);
+void engine_free_bytes(Engine &e, void *p);
 // Neighbour list: thickness >= 0 turns it on (rows within rc + thickness),
 // thickness < 0 off; make rebuilds the cell list and the neighbour list.
 int engine_use_nlist(Engine &e, float thickness);
