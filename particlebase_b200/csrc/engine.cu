@@ -470,6 +470,9 @@ int engine_setup_cells(Engine &e) {
   uint64_t ncells = 0;
   uint32_t mirror = 0;
   e.cap_max = 0;
+  // grids and plans first, so that the item and column arrays are sized once
+  std::vector<std::shared_ptr<const Plan>> plans(e.nsys);
+  size_t nitem_all = 0, ncol_all = 0;
   for (uint32_t s = 0; s < e.nsys; ++s) {
     SysParams &P = e.sp[s];
     if (!P.cell_set) return fail(e, PB_ERR_STATE, "set the cell first");
@@ -481,8 +484,17 @@ int engine_setup_cells(Engine &e) {
     P.seg = choose_segment(apc, g.n[2], e.seg_scale, P.lj_set ? P.lj.nt : 1);
     P.cap = (uint32_t)choose_capacity(apc, P.seg);
     e.cap_max = std::max(e.cap_max, P.cap);
-    const std::shared_ptr<const Plan> plan_ref = cached_plan(g, P.seg);
-    const Plan &plan = *plan_ref;
+    plans[s] = cached_plan(g, P.seg);
+    nitem_all += plans[s]->items.size();
+    ncol_all += plans[s]->rank.size();
+  }
+  items.reserve(nitem_all);
+  rank_all.reserve(ncol_all);
+  xy_all.reserve(ncol_all);
+  for (uint32_t s = 0; s < e.nsys; ++s) {
+    SysParams &P = e.sp[s];
+    const Grid g = P.grid;
+    const Plan &plan = *plans[s];
     const std::vector<uint32_t> &rank = plan.rank, &xy = plan.xy;
     e.cell0[s] = (uint32_t)ncells;
     e.item0[s] = (uint32_t)items.size();

@@ -66,13 +66,19 @@ void neighbor_table(const Grid &g, std::vector<uint32_t> &out) {
       }
 }
 
+// Environment overrides, read once per process.
+static const char *env_once(int slot) {
+  static const char *v[2] = {std::getenv("PB_FORCE_SEG"), std::getenv("PB_FORCE_CAP")};
+  return v[slot];
+}
+
 int choose_segment(double atoms_per_cell, int nz, double scale, int nt) {
   // about 200 home atoms (25 clusters of 8) per force work item; PB_FORCE_SEG
   // overrides.  Shorter runs while the stage would not let two force CTAs
   // share an SM.
   const double apc = std::max(atoms_per_cell, 1.0);
   int seg = (int)std::lround(200.0 * scale / apc);
-  if (const char *e = std::getenv("PB_FORCE_SEG")) seg = std::atoi(e);
+  if (const char *e = env_once(0)) seg = std::atoi(e);
   seg = std::max(1, std::min(seg, force_max_segment()));
   seg = std::min(seg, nz);
   while (seg > 1 && force_smem_per_cta(choose_capacity(apc, seg), nt) > 112 * 1024) --seg;
@@ -82,10 +88,10 @@ int choose_segment(double atoms_per_cell, int nz, double scale, int nt) {
 int choose_capacity(double atoms_per_cell, int seg) {
   const double expect = 9.0 * (seg + 2) * std::max(atoms_per_cell, 1.0);
   double factor = 1.15;  // headroom over the mean occupancy; PB_FORCE_CAP overrides
-  if (const char *e = std::getenv("PB_FORCE_CAP")) factor = std::atof(e);
+  if (const char *e = env_once(1)) factor = std::atof(e);
   const double cap = factor * expect + 128.0;
   // the largest launch shape (8 warps, 8 types) bounds every launch's memory
-  const double max_atoms = (double)force_max_capacity(8, kMaxTypes);
+  static const double max_atoms = (double)force_max_capacity(8, kMaxTypes);
   return (int)std::min(cap, max_atoms);
 }
 
