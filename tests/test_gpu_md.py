@@ -205,6 +205,26 @@ def test_graph_run_equals_eager_steps(cuda_lib):
     assert np.array_equal(a.get("v"), b.get("v"))
 
 
+@pytest.mark.parametrize("gaussian", [False, True])
+def test_temperature_after_steps_reuses_the_step_sum(cuda_lib, gaussian):
+    """calcTemp after a step reads the sum m v^2 that the step's last kernel computed;
+    it must equal the sum recomputed from the same velocities, bit for bit."""
+    s = W.config_c1()
+    p = md(cuda_lib, s, gaussian=gaussian)
+    p.clearForce()
+    for steps in (1, 2, 5):
+        p.run(0.005, steps)
+        t_step = p.calcTemp()           # the step's own sum
+        field = "vd" if gaussian else "v"
+        p.set(field, p.get(field))      # same velocities: the next read recomputes the sum
+        t_fresh = p.calcTemp()
+        assert t_step == t_fresh
+        # the value is the kinetic temperature of the velocities on the host
+        v = p.velocities()
+        t_host = float((s.mass[:, None] * v * v).sum()) / (3 * s.n)
+        assert t_step == pytest.approx(t_host, rel=1e-6)
+
+
 def test_deterministic(cuda_lib):
     s = W.config_c1()
     out = []
