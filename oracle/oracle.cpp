@@ -106,7 +106,8 @@ void neighbor_table(const Grid &g, int periodic, uint32_t *out) {
 // single-CTA sort (sortByBID_M1 + sortByBID + makeBindex,
 // kernelfuncs.cu:844-932): the per-cell member sets and counts are the same;
 // the within-cell order, history-dependent in the reference, is made
-// canonical: ascending FP32 z coordinate, ties by ascending particle id.
+// canonical: ascending FP32 z coordinate, ties by ascending particle id
+// (NaN coordinates last).
 // `z` may be null, giving ascending particle id.
 void cell_list(const uint32_t *cid, const float *z, uint32_t N, uint32_t ncells,
                uint32_t *start, uint32_t *members) {
@@ -116,9 +117,14 @@ void cell_list(const uint32_t *cid, const float *z, uint32_t N, uint32_t ncells,
   std::memcpy(start, cnt.data(), sizeof(uint32_t) * (ncells + 1));
   for (uint32_t i = 0; i < N; ++i) members[cnt[cid[i]]++] = i;
   if (z) {
+    // NaN coordinates sort after every number (ties by id), so the order is
+    // a strict total order whatever the input
+    auto key = [z](uint32_t a) { return std::isnan(z[a]) ? 1 : 0; };
     for (uint32_t c = 0; c < ncells; ++c)
-      std::sort(members + start[c], members + start[c + 1], [z](uint32_t a, uint32_t b) {
-        return z[a] < z[b] || (z[a] == z[b] && a < b);
+      std::sort(members + start[c], members + start[c + 1], [z, key](uint32_t a, uint32_t b) {
+        const int na = key(a), nb = key(b);
+        if (na != nb) return na < nb;
+        return (!na && z[a] < z[b]) || ((na || z[a] == z[b]) && a < b);
       });
   }
 }
@@ -155,6 +161,13 @@ struct ForceOut {
   double ncand = 0, nin = 0;
 };
 
+// Force laws: kLawLJ (the MD step), kLawCapped (relaxation, extension) and
+// kLawSoftCore, the soft-core repulsion of initialAnnealing
+// (cudaParticleMD.cu:205-262): potentialSC (kernelinline.hh:136-158) gives
+// f0 cos(r / rc_sc * pi / 2), zero for r > rc_sc, which MDpairForce applies
+// along (r_i - r_j) / r for pairs inside the LJ cutoff.
+enum ForceLaw { kLawLJ = 0, kLawCapped = 1, kLawSoftCore = 2 };
+
 // Pair force of MDpairForce<potentialLJ> (kerneltemplate.hh:530-564,
 // kernelinline.hh:86-96) in FP64: F_i = sum_j 24 eps (s/r)^6 (2 (s/r)^6 - 1)/r^2
 // * (r_i - r_j), minimum image, truncated at rc, unshifted.  Enumerates the
@@ -164,7 +177,9 @@ struct ForceOut {
 void compute_forces(const double *r3, const uint32_t *type, uint32_t N, const double *L,
                     const Grid &g, const uint32_t *nbr, const uint32_t *start,
                     const uint32_t *members, const uint32_t *cid, const LJTable &t,
-                    double *F3, double *pe_atom, ForceOut &out, bool capped = false) {
+                    double *F3, double *pe_atom, ForceOut &out, int law = kLawLJ,
+                    double sc_rc = 0, double sc_f0 = 0) {
+  const bool capped = law == kLawCapped;
   double pe = 0, pes = 0, vir = 0, nc = 0, ni = 0;
   const int nt = t.ntypes;
 #pragma omp parallel for schedule(dynamic, 64) reduction(+ : pe, pes, vir, nc, ni)
@@ -187,6 +202,16 @@ void compute_forces(const double *r3, const uint32_t *type, uint32_t N, const do
         if (dz > 0.5 * L[2]) dz -= L[2]; else if (dz < -0.5 * L[2]) dz += L[2];
         const double r2 = dx * dx + dy * dy + dz * dz;
         const int k = ti * nt + (int)type[j];
+        if (law == kLawSoftCore) {
+          const double r = std::sqrt(r2);
+          if (r2 < t.rc2[k] && r <= sc_rc) {
+            const double f = sc_f0 * std::cos(r / sc_rc * M_PI / 2) / r;
+            fx += f * dx;
+            fy += f * dy;
+            fz += f * dz;
+          }
+          continue;
+        }
         if (r2 < t.rc2[k]) {
           ni += 1;
           // relaxation force (extension): r^2 floored at (sigma/2)^2 so that
@@ -254,10 +279,11 @@ void build_cells(System &s) {
   cell_list(cid.data(), nullptr, s.N, s.g.ncells, s.start.data(), s.members.data());
 }
 
-void forces(System &s, bool capped = false) {
+void forces(System &s, int law = kLawLJ, double sc_rc = 0, double sc_f0 = 0) {
   build_cells(s);
   compute_forces(s.r.data(), s.type.data(), s.N, s.L, s.g, s.nbr.data(), s.start.data(),
-                 s.members.data(), s.cid.data(), s.t, s.F.data(), s.pe_atom.data(), s.fo, capped);
+                 s.members.data(), s.cid.data(), s.t, s.F.data(), s.pe_atom.data(), s.fo, law,
+                 sc_rc, sc_f0);
 }
 
 void wrap_all(System &s) {
@@ -521,7 +547,7 @@ int orc_run(void *h, uint32_t steps, double dt, int mode, double *energy_out) {
 void orc_steepest_descent(void *h, uint32_t iters, double alpha, double max_disp) {
   System &s = *(System *)h;
   for (uint32_t it = 0; it < iters; ++it) {
-    forces(s, true);
+    forces(s, kLawCapped);
 #pragma omp parallel for schedule(static)
     for (long i = 0; i < (long)s.N; ++i) {
       const double fx = s.F[3 * i], fy = s.F[3 * i + 1], fz = s.F[3 * i + 2];
@@ -533,6 +559,93 @@ void orc_steepest_descent(void *h, uint32_t iters, double alpha, double max_disp
     }
     wrap_all(s);
   }
+}
+
+// adjustVelocity_F4 / adjustVelocity_VD (kernelfuncs.cu:546-699), called by
+// adjustVelocities (cudaParticleMD.cu:177-198, GaussianThermo.cu:98-119):
+// per axis, FP64 mean and variance over all atoms, then
+// v = (v - mean) * v1 / sqrt(variance).
+void orc_adjust_velocities(void *h, double v1) {
+  System &s = *(System *)h;
+  double m[3] = {0, 0, 0}, q[3] = {0, 0, 0};
+  for (uint32_t i = 0; i < s.N; ++i)
+    for (int k = 0; k < 3; ++k) {
+      m[k] += s.v[3 * i + k];
+      q[k] += s.v[3 * i + k] * s.v[3 * i + k];
+    }
+  double f[3];
+  for (int k = 0; k < 3; ++k) {
+    m[k] /= s.N;
+    f[k] = v1 / std::sqrt(q[k] / s.N - m[k] * m[k]);
+  }
+  for (uint32_t i = 0; i < s.N; ++i)
+    for (int k = 0; k < 3; ++k) s.v[3 * i + k] = (s.v[3 * i + k] - m[k]) * f[k];
+}
+
+// scaleTemp (cudaParticleMD.cu:168-175, GaussianThermo.cu:89-96): T0 = sum m
+// v^2 / (3 N kB), v *= sqrt((3N - 1) / (3N) T / T0).  Returns the factor.
+double orc_scale_temp(void *h, double T, double kB) {
+  System &s = *(System *)h;
+  const double T0 = sum_mv2(s) / (3.0 * s.N * kB);
+  const double f = std::sqrt((3.0 * s.N - 1) / (3.0 * s.N) * T / T0);
+  for (double &x : s.v) x *= f;
+  return f;
+}
+
+// Soft-core force of initialAnnealing (see kLawSoftCore) at the current
+// positions.
+void orc_forces_softcore(void *h, double rc, double f0) {
+  System &s = *(System *)h;
+  forces(s, kLawSoftCore, rc, f0);
+}
+
+// constTemp (cudaParticleMD.cu:140-155) with correctConstTemp_F4
+// (kernelfuncs.cu:533-544): lambda = sum F.v / sum m v^2, F -= lambda m v.
+// Returns lambda.
+double orc_const_temp(void *h) {
+  System &s = *(System *)h;
+  const double lam = sum_fv(s) / sum_mv2(s);
+  if (lam != 0)
+    for (uint32_t i = 0; i < s.N; ++i)
+      for (int k = 0; k < 3; ++k) s.F[3 * i + k] -= lam * s.mass[i] * s.v[3 * i + k];
+  return lam;
+}
+
+// The Euler step of initialAnnealing (cudaParticleMD.cu:271-277): calcA_F4
+// (kernelfuncs.cu:70-82), propagateEuler_F4 (kernelfuncs.cu:174-192: r += v dt
+// with the old v, then v += a dt) and the periodic wrap.
+void orc_euler(void *h, double dt) {
+  System &s = *(System *)h;
+  for (uint32_t i = 0; i < s.N; ++i)
+    for (int k = 0; k < 3; ++k) {
+      const size_t q = 3 * i + k;
+      s.r[q] += s.v[q] * dt;
+      s.v[q] += s.F[q] / s.mass[i] * dt;
+    }
+  wrap_all(s);
+}
+
+// cudaParticleMD::initialAnnealing (cudaParticleMD.cu:205-325): anealstep
+// soft-core Euler steps with the range growing to rc (rc (i + 1) / anealstep),
+// each with constTemp; a rescale to T; Fold cleared; anealstep LJ
+// velocity-Verlet steps with constTemp; a final rescale.
+void orc_initial_annealing(void *h, uint32_t anealstep, double dt, double rc, double f0,
+                           double T, double kB) {
+  System &s = *(System *)h;
+  for (uint32_t i = 0; i < anealstep; ++i) {
+    forces(s, kLawSoftCore, rc * (i + 1) / anealstep, f0);
+    orc_const_temp(h);
+    orc_euler(h, dt);
+  }
+  orc_scale_temp(h, T, kB);
+  std::fill(s.Fold.begin(), s.Fold.end(), 0.0);
+  for (uint32_t i = 0; i < anealstep; ++i) {
+    forces(s);
+    orc_const_temp(h);
+    step_vv(s, dt);
+    wrap_all(s);
+  }
+  orc_scale_temp(h, T, kB);
 }
 
 double orc_kinetic(void *h) { return 0.5 * sum_mv2(*(System *)h); }

@@ -77,6 +77,15 @@ def lib() -> C.CDLL:
         L.orc_get_nr_iters.argtypes = [C.c_void_p]
         L.orc_get.argtypes = [C.c_void_p, C.c_int, _f64p]
         L.orc_threads.restype = C.c_int
+        L.orc_adjust_velocities.argtypes = [C.c_void_p, C.c_double]
+        L.orc_scale_temp.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.orc_scale_temp.restype = C.c_double
+        L.orc_forces_softcore.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.orc_const_temp.argtypes = [C.c_void_p]
+        L.orc_const_temp.restype = C.c_double
+        L.orc_euler.argtypes = [C.c_void_p, C.c_double]
+        L.orc_initial_annealing.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double,
+                                            C.c_double, C.c_double, C.c_double]
         _lib = L
     return _lib
 
@@ -116,6 +125,17 @@ def ref() -> C.CDLL:
         L.ref_threads.restype = C.c_int
         L.ref_gr.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_uint32]
         L.ref_gr.restype = C.c_int
+        L.ref_adjust_velocities.argtypes = [C.c_void_p, C.c_float]
+        L.ref_scale_temp.argtypes = [C.c_void_p, C.c_float]
+        L.ref_scale_temp.restype = C.c_double
+        L.ref_calc_force_softcore.argtypes = [C.c_void_p, C.c_float, C.c_float]
+        L.ref_const_temp.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.ref_const_temp.restype = C.c_double
+        L.ref_euler.argtypes = [C.c_void_p, C.c_float]
+        L.ref_initial_annealing.argtypes = [C.c_void_p, C.c_uint32, C.c_float, C.c_float,
+                                            C.c_float, C.c_float]
+        L.ref_set_v.argtypes = [C.c_void_p, _f32p]
+        L.ref_set_F.argtypes = [C.c_void_p, _f32p]
         _ref = L
     return _ref
 
@@ -219,6 +239,29 @@ class Oracle:
         with the relaxation force (pair distance floored at sigma/2)."""
         lib().orc_steepest_descent(self.h, iters, alpha, max_disp)
 
+    def adjust_velocities(self, v1):
+        """adjustVelocity_F4 / _VD: zero mean, standard deviation v1 per axis."""
+        lib().orc_adjust_velocities(self.h, v1)
+
+    def scale_temp(self, T, kB=1.0):
+        """scaleTemp: returns the factor sqrt((3N-1)/(3N) T/T0) applied to v."""
+        return lib().orc_scale_temp(self.h, T, kB)
+
+    def forces_softcore(self, rc, f0):
+        """The soft-core force of initialAnnealing (potentialSC)."""
+        lib().orc_forces_softcore(self.h, rc, f0)
+
+    def const_temp(self):
+        """constTemp's correction F -= lambda m v; returns lambda."""
+        return lib().orc_const_temp(self.h)
+
+    def euler(self, dt):
+        """calcA_F4 + propagateEuler_F4 + wrap."""
+        lib().orc_euler(self.h, dt)
+
+    def initial_annealing(self, steps, dt, rc, f0, T, kB=1.0):
+        lib().orc_initial_annealing(self.h, steps, dt, rc, f0, T, kB)
+
     def get(self, name):
         idx = {"r": 0, "v": 1, "F": 2, "Fold": 3, "pe_atom": 4}[name]
         out = np.zeros(self.N if name == "pe_atom" else 3 * self.N)
@@ -278,6 +321,34 @@ class RefKernels:
 
     def mv2(self):
         return ref().ref_calc_mv2(self.h)
+
+    def adjust_velocities(self, v1):
+        """adjustVelocity_F4 / adjustVelocity_VD with v1 = sqrt(kB T / m0) (FP32)."""
+        ref().ref_adjust_velocities(self.h, v1)
+
+    def scale_temp(self, T):
+        """scaleTemp: returns the factor applied (mulArray)."""
+        return ref().ref_scale_temp(self.h, T)
+
+    def calc_force_softcore(self, rc, f0):
+        """Soft-core force of initialAnnealing (potentialSC) on the current cells."""
+        ref().ref_calc_force_softcore(self.h, rc, f0)
+
+    def const_temp(self):
+        """constTemp: returns (temperature, lambda); corrects F when lambda != 0."""
+        lam = C.c_double()
+        t = ref().ref_const_temp(self.h, C.byref(lam))
+        return t, lam.value
+
+    def euler(self, dt):
+        """calcA_F4 + propagateEuler_F4 + applyPeriodicCondition_F4."""
+        ref().ref_euler(self.h, dt)
+
+    def initial_annealing(self, steps, dt, rc, f0, T):
+        ref().ref_initial_annealing(self.h, steps, dt, rc, f0, T)
+
+    def set4(self, name, arr):
+        getattr(ref(), "ref_set_" + name)(self.h, np.ascontiguousarray(arr, np.float32).reshape(-1))
 
     def get4(self, name):
         out = np.zeros(4 * self.N, np.float32)

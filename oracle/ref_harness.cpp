@@ -337,6 +337,139 @@ void ref_wrap(void *h) {
   launch(dim3(threads1D(s)), true, applyPeriodicCondition_F4, s.r.data(), c1, c2, s.N);
 }
 
+// cudaParticleMD::adjustVelocities (cudaParticleMD.cu:177-198) and
+// GaussianThermo::adjustVelocities (GaussianThermo.cu:98-119): the reference
+// launches adjustVelocity_F4 / adjustVelocity_VD (kernelfuncs.cu:546-699) as
+// one block of min(1024, threadsMax) threads.  Here the same kernel runs as
+// one thread (st = 1): the per-axis sums are the same FP64 sums added in
+// sequence instead of by the block's tree.  v1 is the caller's
+// sqrt(kB T / m0) in `real`, as the reference computes it.
+void ref_adjust_velocities(void *h, float v1) {
+  RefSys &s = *(RefSys *)h;
+  if (s.gaussian)
+    launch(dim3(1), false, adjustVelocity_VD, s.vd.data(), (uint32_t)1, s.N, (real)v1,
+           (float *)nullptr);
+  else
+    launch(dim3(1), false, adjustVelocity_F4, s.v.data(), (uint32_t)1, s.N, (real)v1,
+           (float *)nullptr);
+}
+
+// cudaParticleMD::scaleTemp (cudaParticleMD.cu:168-175; FP32 factor, mulArray
+// over the 4 N floats of v) and GaussianThermo::scaleTemp (GaussianThermo.cu:89-96;
+// FP64 factor over the 3 N doubles of vd).  T0 is calcTemp()
+// (cudaParticleMD.hh:89-92) = calcMV2 / (3 N kB).  Returns the factor.
+double ref_scale_temp(void *h, float T) {
+  RefSys &s = *(RefSys *)h;
+  const uint32_t Tn = threads1D(s);
+  const real mv2 = s.gaussian ? gauss_mv2(s) : vv_mv2(s);
+  const real T0 = mv2 / (s.N * 3 * s.kB);
+  if (s.gaussian) {
+    const double f = sqrt(static_cast<double>(3 * s.N - 1) / static_cast<double>(3 * s.N) * T / T0);
+    launch(dim3(Tn), true, mulArray<double>, s.vd.data(), f, s.N * 3);
+    return f;
+  }
+  const real f = sqrt(static_cast<real>(3 * s.N - 1) / static_cast<real>(3 * s.N) * T / T0);
+  launch(dim3(Tn), true, mulArray<float>, reinterpret_cast<float *>(s.v.data()), f, s.N * 4);
+  return f;
+}
+
+// The soft-core force of initialAnnealing (cudaParticleMD.cu:226-262):
+// calcF_IJpairWithBlock_F4<MDpairForce<potentialSC>> (kerneltemplate.hh:229-294,
+// 523-565; potentialSC kernelinline.hh:136-158) + reduce27_F4 on the current
+// cell list, with P.rmax2 the LJ cutoff and op.rc, op.f0 as given.
+void ref_calc_force_softcore(void *h, float rc, float f0) {
+  RefSys &s = *(RefSys *)h;
+  const uint32_t T = threads1D(s);
+  launch(dim3(T), true, clearArray_F4, s.F.data(), s.N, float4{0, 0, 0, 0});
+  potentialSC SC;
+  SC.rc = rc;
+  SC.f0 = f0;
+  MDpairForce<potentialSC> P;
+  P.cx = s.cell[6];
+  P.cy = s.cell[7];
+  P.cz = s.cell[8];
+  P.c0x = sqrt(P.cx) * 2.0;
+  P.c0y = sqrt(P.cy) * 2.0;
+  P.c0z = sqrt(P.cz) * 2.0;
+  P.rmax2 = s.rmax2;
+  P.typeID = s.typeID_s.data();
+  P.op = SC;
+  launch(dim3(T), true, clearArray<real>, s.tmp81N.data(), s.N * 81, (real)0);
+  launch(dim3(s.totalNumBlock, 27), true, calcF_IJpairWithBlock_F4<MDpairForce<potentialSC>>,
+         P, s.r_s.data(), s.tmp81N.data(), (uint32_t)0, s.blockNeighbor.data(), s.pid.data(),
+         s.bindex.data(), s.N, (real *)nullptr, (uint32_t *)nullptr, true, false);
+  launch(dim3(T), true, reduce27_F4, s.F.data(), s.tmp81N.data(), s.N);
+}
+
+// cudaParticleMD::constTemp (cudaParticleMD.cu:140-155): lambda = sum F.v /
+// sum m v^2 over the 4 N floats (cublasSdot replaced by a sequential FP32
+// dot product, as in vv_mv2), then correctConstTemp_F4 (kernelfuncs.cu:533-544)
+// when lambda != 0.  Returns the temperature t / (3 N kB); *lambda_out = lambda.
+double ref_const_temp(void *h, double *lambda_out) {
+  RefSys &s = *(RefSys *)h;
+  const real t = vv_mv2(s);
+  real lambda = 0;
+  const float *F = reinterpret_cast<const float *>(s.F.data());
+  const float *v = reinterpret_cast<const float *>(s.v.data());
+  for (uint32_t i = 0; i < 4 * s.N; ++i) lambda += F[i] * v[i];
+  lambda /= t;
+  if (lambda != 0)
+    launch(dim3(threads1D(s)), true, correctConstTemp_F4, s.v.data(), s.F.data(), s.m.data(),
+           lambda, s.N);
+  if (lambda_out) *lambda_out = lambda;
+  return t / (3 * s.N * s.kB);
+}
+
+// The Euler step of initialAnnealing (cudaParticleMD.cu:271-277): calcA_F4
+// (kernelfuncs.cu:70-82) into a, propagateEuler_F4 (kernelfuncs.cu:174-192)
+// with every particle movable (move[i] = 1), applyPeriodicCondition_F4.
+void ref_euler(void *h, float dt) {
+  RefSys &s = *(RefSys *)h;
+  const uint32_t T = threads1D(s);
+  std::vector<char> move(s.N, 1);
+  launch(dim3(T), true, calcA_F4, s.a.data(), s.minv.data(), s.F.data(), s.N);
+  launch(dim3(T), true, propagateEuler_F4, s.r.data(), (real)dt, s.v.data(), s.a.data(),
+         move.data(), s.N);
+  ref_wrap(h);
+}
+
+// cudaParticleMD::initialAnnealing (cudaParticleMD.cu:205-325) for the plain
+// MD class: anealstep soft-core Euler steps whose range grows to rc, a
+// temperature rescale, anealstep LJ velocity-Verlet steps with constTemp, and
+// a final rescale.  The second stage clears Fold (cudaParticleMD.cu:289).
+void ref_initial_annealing(void *h, uint32_t anealstep, float dt, float rc, float f0, float T) {
+  RefSys &s = *(RefSys *)h;
+  const uint32_t Tn = threads1D(s);
+  for (uint32_t i = 0; i < anealstep; ++i) {
+    const real rci = rc * (i + 1) / anealstep;
+    ref_calc_block_id(h);
+    ref_calc_force_softcore(h, rci, f0);
+    ref_const_temp(h, nullptr);
+    ref_euler(h, dt);
+  }
+  ref_scale_temp(h, T);
+  launch(dim3(Tn), true, clearArray_F4, s.a.data(), s.N, float4{0, 0, 0, 0});
+  for (uint32_t i = 0; i < anealstep; ++i) {
+    ref_calc_block_id(h);
+    ref_calc_force(h);
+    ref_const_temp(h, nullptr);
+    launch(dim3(Tn), true, propagateVelocityVerlet_F4, s.r.data(), (real)dt, s.v.data(),
+           s.F.data(), s.a.data(), s.minv.data(), s.N);
+    ref_wrap(h);
+  }
+  ref_scale_temp(h, T);
+}
+
+void ref_set_v(void *h, const float *v4) {
+  RefSys &s = *(RefSys *)h;
+  std::memcpy(s.v.data(), v4, sizeof(float4) * s.N);
+}
+
+void ref_set_F(void *h, const float *F4) {
+  RefSys &s = *(RefSys *)h;
+  std::memcpy(s.F.data(), F4, sizeof(float4) * s.N);
+}
+
 // Driver order of testMD2.cu:149-168 / testMD1.cu:135-154 without the
 // temperature policy: calcBlockID, calcForce, TimeEvolution, PBC.
 int ref_run(void *h, float dt, uint32_t steps) {

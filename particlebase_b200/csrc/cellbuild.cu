@@ -154,8 +154,20 @@ __device__ __forceinline__ void write_mirror(const CellBufs &b, uint32_t me, uin
   b.ts[m] = (uint32_t)b.type[me];
 }
 
-__device__ __forceinline__ bool canon_before(float za, uint32_t a, float zb, uint32_t b) {
-  return za < zb || (za == zb && a < b);
+// Order key of a z coordinate: monotone in z for all non-NaN values (-0 and
+// +0 share a key, as they compare equal), every NaN after +Inf.  Ranking by
+// (key, particle id) is a strict total order, so the ranks of a cell's members
+// are a permutation of 0 .. n - 1 even when a coordinate is NaN: no slot is
+// left unwritten and none is written twice.
+__device__ __forceinline__ uint32_t z_key(float z) {
+  if (z != z) return 0xffffffffu;
+  uint32_t u = __float_as_uint(z);
+  if (u == 0x80000000u) u = 0u;
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__device__ __forceinline__ bool canon_before(uint32_t ka, uint32_t a, uint32_t kb, uint32_t b) {
+  return ka < kb || (ka == kb && a < b);
 }
 
 // Rank of every member of one cell by (z, particle id), one lane per member,
@@ -166,11 +178,12 @@ __device__ __forceinline__ void canon_cell(const CellBufs &b, uint32_t s0, uint3
                                            int base, uint32_t lanes_n) {
   const uint32_t me = li < (int)n ? b.pid_tmp[s0 + li] : kNone;
   const float4 p = li < (int)n ? b.r[me] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const uint32_t kz = z_key(p.z);
   uint32_t rank = 0;
   for (uint32_t k = 0; k < lanes_n; ++k) {
     const uint32_t other = __shfl_sync(0xffffffffu, me, base + (int)k);
-    const float zo = __shfl_sync(0xffffffffu, p.z, base + (int)k);
-    rank += (k < n && canon_before(zo, other, p.z, me)) ? 1u : 0u;
+    const uint32_t ko = __shfl_sync(0xffffffffu, kz, base + (int)k);
+    rank += (k < n && canon_before(ko, other, kz, me)) ? 1u : 0u;
   }
   if (li < (int)n) {
     const uint32_t s = s0 + rank;
@@ -186,10 +199,11 @@ __device__ void canon_large(const CellBufs &b, uint32_t s0, uint32_t n, int lane
   for (uint32_t a = lane; a < n; a += 32) {
     const uint32_t me = b.pid_tmp[s0 + a];
     const float4 p = b.r[me];
+    const uint32_t kz = z_key(p.z);
     uint32_t rank = 0;
     for (uint32_t k = 0; k < n; ++k) {
       const uint32_t other = b.pid_tmp[s0 + k];
-      rank += canon_before(b.r[other].z, other, p.z, me) ? 1u : 0u;
+      rank += canon_before(z_key(b.r[other].z), other, kz, me) ? 1u : 0u;
     }
     const uint32_t s = s0 + rank;
     b.pid[s] = me;

@@ -16,6 +16,15 @@
 // one scratch array, so calls that overlap on the GPU (different streams, or
 // different host threads) race; serialise them.  The per-cell counters are
 // cleared at the start of every call.
+//
+// The call is stream-ordered and returns without waiting for the GPU: the
+// system descriptor and the column ranks travel to the scratch array as
+// kernel parameters (copied at launch), so no host memory of the call is read
+// after it returns.  The scratch array's device address is resolved once per
+// device (cudaGetSymbolAddress) and cached; that address belongs to the
+// context the first call ran in, so use one context per device (the primary
+// context, as the CUDA runtime does) and do not reset the device between calls.
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -67,6 +76,21 @@ cudaError_t scratch_on_current_device(ScratchLayout **out) {
   return cudaSuccess;
 }
 
+// Host values handed to the GPU as kernel parameters: up to kChunk column
+// ranks per launch (16 KB of parameters, well inside the 32 KB launch limit),
+// and the system descriptor.
+constexpr uint32_t kChunk = 4096;
+struct RankChunk {
+  uint32_t first, n;
+  uint32_t v[kChunk];
+};
+
+__global__ void k_put_ranks(const RankChunk c, uint32_t *dst) {
+  for (uint32_t i = threadIdx.x; i < c.n; i += blockDim.x) dst[c.first + i] = c.v[i];
+}
+
+__global__ void k_put_sys(const SysDesc sd, SysDesc *dst) { *dst = sd; }
+
 }  // namespace
 }  // namespace pb
 
@@ -92,17 +116,26 @@ extern "C" int pb_cells_build_noalloc(const void *r4, const uint16_t *type, uint
   if (scratch_on_current_device(&sc) != cudaSuccess) return PB_ERR_CUDA;
   cudaStream_t s = (cudaStream_t)stream;
 
-  // Host-side tables: system descriptor and Z-order column ranks (copied,
-  // from pageable host memory, into the static scratch).
+  // Host-side tables: system descriptor and Z-order column ranks, written
+  // into the static scratch by kernels that carry them as parameters.
   std::vector<uint32_t> rank, xy;
   morton_columns(g.n[0], g.n[1], rank, xy);
   SysDesc sd{};
   sd.g = g;
   sd.natoms = n;
-  if (cudaMemcpyAsync(&sc->sys, &sd, sizeof(SysDesc), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(sc->colrank, rank.data(), sizeof(uint32_t) * rank.size(),
-                      cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemsetAsync(sc->count, 0, sizeof(uint32_t) * g.ncells, s) != cudaSuccess)
+  k_put_sys<<<1, 1, 0, s>>>(sd, &sc->sys);
+  if (cudaGetLastError() != cudaSuccess) return PB_ERR_CUDA;
+  {
+    RankChunk c;  // ~16 KB on the host stack, copied into the launch
+    for (uint32_t first = 0; first < (uint32_t)rank.size(); first += kChunk) {
+      c.first = first;
+      c.n = std::min<uint32_t>(kChunk, (uint32_t)rank.size() - first);
+      std::copy(rank.begin() + first, rank.begin() + first + c.n, c.v);
+      k_put_ranks<<<1, 256, 0, s>>>(c, sc->colrank);
+      if (cudaGetLastError() != cudaSuccess) return PB_ERR_CUDA;
+    }
+  }
+  if (cudaMemsetAsync(sc->count, 0, sizeof(uint32_t) * g.ncells, s) != cudaSuccess)
     return PB_ERR_CUDA;
   if (!type && cudaMemsetAsync(sc->type0, 0, sizeof(uint16_t) * n, s) != cudaSuccess)
     return PB_ERR_CUDA;
@@ -125,8 +158,6 @@ extern "C" int pb_cells_build_noalloc(const void *r4, const uint16_t *type, uint
   b.slot = slot;
   b.rs = reinterpret_cast<float4 *>(rs4);
   b.status = nullptr;
-  // The host copies above read stack/vector memory: finish them before return.
   if (launch_cell_build(b, s) != cudaSuccess) return PB_ERR_CUDA;
-  if (cudaStreamSynchronize(s) != cudaSuccess) return PB_ERR_CUDA;
   return PB_OK;
 }

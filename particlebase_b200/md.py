@@ -245,16 +245,69 @@ class MDSystem:
         return self.sums()["pe"]
 
     def scaleTemp(self, temp: float) -> float:
+        """scaleTemp (cudaParticleMD.cu:168-175, GaussianThermo.cu:89-96): v *= s,
+        s = sqrt((3N-1)/(3N) T/T0); FP32 arithmetic for the plain class, FP64 for
+        the Gaussian one, as the reference computes it."""
         t0 = self.calcTemp()
-        s = np.sqrt((3 * self.n - 1) / (3 * self.n) * temp / t0)
+        if self.gaussian:
+            s = float(np.sqrt((3 * self.n - 1) / (3 * self.n) * float(np.float32(temp))
+                              / float(np.float32(t0))))
+        else:
+            f32 = np.float32
+            s = float(np.sqrt(f32(3 * self.n - 1) / f32(3 * self.n) * f32(temp) / f32(t0),
+                              dtype=np.float32))
         self._ck(self.lib.pb_md_scale_velocities(self.h, C.c_double(s)), "scale")
         return float(s)
 
     def adjustVelocities(self, temp: float, debug: bool = False) -> None:
+        """cudaParticleMD::adjustVelocities (cudaParticleMD.cu:177-198): zero mean
+        and standard deviation v1 = sqrt(kB T / m0) per axis, v1 in FP32 as the
+        reference computes it."""
         m0 = C.c_double()
         self._ck(self.lib.pb_md_mean_mass(self.h, C.byref(m0)), "mean_mass")
-        v1 = np.sqrt(self._kB * temp / m0.value)
-        self._ck(self.lib.pb_md_adjust_velocities(self.h, C.c_double(v1)), "adjust")
+        v1 = np.sqrt(np.float32(self._kB) * np.float32(temp) / np.float32(m0.value),
+                     dtype=np.float32)
+        self._ck(self.lib.pb_md_adjust_velocities(self.h, C.c_double(float(v1))), "adjust")
+
+    def constTemp(self) -> float:
+        """cudaParticleMD::constTemp (cudaParticleMD.cu:140-155): lambda =
+        sum F.v / sum m v^2 (FP64 sums), F -= lambda m v; returns the temperature."""
+        s = self.sums()
+        lam = s["fv"] / s["mv2"] if s["mv2"] > 0 else 0.0
+        if lam != 0:
+            self._ck(self.lib.pb_md_correct_force(self.h, C.c_double(lam)), "correct_force")
+        return float(np.float32(s["mv2"])) / (3 * self.n * self._kB)
+
+    def calcForceSoftCore(self, rc: float, f0: float) -> None:
+        """The soft-core force of initialAnnealing (potentialSC, kernelinline.hh:136-158)
+        on the current cell list."""
+        self._ck(self.lib.pb_md_force_softcore(self.h, C.c_float(rc), C.c_float(f0)),
+                 "force_softcore")
+
+    def stepEuler(self, dt: float) -> None:
+        """calcA_F4 + propagateEuler_F4 + applyPeriodicCondition_F4 with the latest force."""
+        self._ck(self.lib.pb_md_step_euler(self.h, C.c_float(dt)), "step_euler")
+
+    def initialAnnealing(self, anealstep: int, dt: float, rc: float, f0: float, T: float) -> None:
+        """cudaParticleMD::initialAnnealing (cudaParticleMD.cu:205-325): anealstep
+        soft-core Euler steps with the range growing to rc, each with constTemp,
+        a rescale to T, anealstep LJ velocity-Verlet steps with constTemp, and a
+        final rescale."""
+        for i in range(anealstep):
+            rci = float(np.float32(np.float32(rc) * np.float32(i + 1)) / np.float32(anealstep))
+            self.calcBlockID()
+            self.calcForceSoftCore(rci, f0)
+            self.constTemp()
+            self.stepEuler(dt)
+        self.scaleTemp(T)
+        self.clearForce()
+        for _ in range(anealstep):
+            self.calcBlockID()
+            self.calcForce()
+            self.constTemp()
+            self._ck(self.lib.pb_md_step_vv(self.h, C.c_float(dt)), "step_vv")
+            self.treatPeriodicCondition()
+        self.scaleTemp(T)
 
     def status(self) -> int:
         b = C.c_uint32()

@@ -4,8 +4,10 @@ The reference (particlelover/ParticleBase) ships no unit tests or fixtures.
 This script runs its kernels -- compiled for the CPU into oracle/_ref by
 oracle/Makefile (calcBID_F4, the sortByBID family, makeBindex,
 calc_BlockNeighbor, calcF_IJpairWithBlock_F4<MDpairForce<potentialLJ>> +
-reduce27_F4, propagateVelocityVerlet_F4, the Gaussian-thermostat kernels and
-applyPeriodicCondition_F4) -- on small seeded inputs and stores the outputs in
+reduce27_F4, propagateVelocityVerlet_F4, the Gaussian-thermostat kernels,
+applyPeriodicCondition_F4, adjustVelocity_F4 / adjustVelocity_VD, mulArray
+(scaleTemp), MDpairForce<potentialSC>, correctConstTemp_F4, calcA_F4 and
+propagateEuler_F4 of initialAnnealing) -- on small seeded inputs and stores the outputs in
 tests/golden/*.npz.  The oracle is checked against these files in
 tests/test_oracle.py, so the pin holds where the reference checkout is absent.
 
@@ -147,6 +149,55 @@ def main() -> None:
     out["gr_r4"] = Rg.get4("r")
     out["gr_rstep_rmax"] = np.array([0.05, 4.0], np.float32)
     out["gr_counts"] = Rg.gr_counts(0.05, 4.0)
+
+    # 10. velocity initialisation and rescaling (adjustVelocity_F4 / _VD,
+    # scaleTemp with mulArray) on 4,000 atoms whose velocities have a nonzero
+    # mean and unequal spreads per axis.  v1 = sqrt(kB T / m0) in FP32, T 0.72.
+    rng = np.random.default_rng(21)
+    v_raw = rng.normal([0.3, -0.2, 0.1], [1.0, 0.7, 1.3], (s.n, 3)).astype(np.float32)
+    v1 = float(np.sqrt(np.float32(1.0) * np.float32(0.72) / np.float32(1.0), dtype=np.float32))
+    out["vel_in"] = v_raw
+    out["vel_v1_T"] = np.array([v1, 0.72], np.float64)
+    Ra = po.RefKernels(s.box, s.rc, r, v_raw.astype(np.float64), s.mass, s.types, [1.0, 1.0])
+    Ra.adjust_velocities(v1)
+    out["adjust_vv_v4"] = Ra.get4("v")
+    Rb = po.RefKernels(s.box, s.rc, r, v_raw.astype(np.float64), s.mass, s.types, [1.0, 1.0],
+                       gaussian=True)
+    Rb.adjust_velocities(v1)
+    out["adjust_gauss_vd"] = Rb.vd()
+    # scaleTemp to T = 1.1 from the raw velocities
+    Rc = po.RefKernels(s.box, s.rc, r, v_raw.astype(np.float64), s.mass, s.types, [1.0, 1.0])
+    fvv = Rc.scale_temp(1.1)
+    out["scale_vv_v4"] = Rc.get4("v")
+    Rd = po.RefKernels(s.box, s.rc, r, v_raw.astype(np.float64), s.mass, s.types, [1.0, 1.0],
+                       gaussian=True)
+    fg = Rd.scale_temp(1.1)
+    out["scale_gauss_vd"] = Rd.vd()
+    out["scale_factors"] = np.array([fvv, fg], np.float64)
+
+    # 11. initialAnnealing's pieces on the perturbed C1 snapshot with the
+    # MB velocities: the soft-core force (range 1.2, strength 1.0), constTemp's
+    # correction of it, and one Euler step (dt 0.005) with the corrected force.
+    Rs = ref_system(s, r)
+    Rs.calc_block_id()
+    Rs.calc_force_softcore(1.2, 1.0)
+    out["sc_rc_f0_dt"] = np.array([1.2, 1.0, 0.005], np.float64)
+    out["sc_F"] = Rs.get4("F")
+    t_ct, lam = Rs.const_temp()
+    out["sc_consttemp_T_lambda"] = np.array([t_ct, lam], np.float64)
+    out["sc_F_corrected"] = Rs.get4("F")
+    Rs.euler(0.005)
+    out["sc_euler_r4"] = Rs.get4("r")
+    out["sc_euler_v4"] = Rs.get4("v")
+
+    # 12. a short initialAnnealing: 5 soft-core Euler steps with the range
+    # growing to 1.2 (f0 1.0, dt 0.005), rescale to T 0.72, 5 LJ VV steps with
+    # constTemp, rescale.
+    Rn = ref_system(s, r)
+    Rn.initial_annealing(5, 0.005, 1.2, 1.0, 0.72)
+    out["anneal_args"] = np.array([5, 0.005, 1.2, 1.0, 0.72], np.float64)
+    out["anneal_r4"] = Rn.get4("r")
+    out["anneal_v4"] = Rn.get4("v")
 
     path = os.path.join(HERE, "reference_kernels.npz")
     np.savez_compressed(path, **out)

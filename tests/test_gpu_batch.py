@@ -193,3 +193,37 @@ def test_step_budgets_stop_each_system_exactly(cuda_lib):
             assert_same(b.get(k, vf), p.get(vf), f"system {k} velocities")
             assert_same(b.get(k, "F"), p.get("F"), f"system {k} last force")
         b.close()
+
+
+@pytest.mark.parametrize("gaussian", [False, True])
+def test_nonfinite_replica_is_isolated(cuda_lib, gaussian):
+    """Failure detection made on the host: one atom of the middle replica gets a
+    NaN velocity before import (the reference drivers stop on a NaN temperature,
+    testMD2.cu:157-163).  Only that replica raises PB_STATUS_NONFINITE; the
+    others stay bit-identical to their runs alone, and the NaN atom's position,
+    binned to cell 0 of its own box, breaks no cell list."""
+    import copy
+
+    from particlebase_b200.batch import Batch
+    systems = replicas(3, seed=31, n_hi=3000)
+    bad = copy.deepcopy(systems[1])
+    bad.v = bad.v.copy()
+    bad.v[0, 0] = np.nan
+    b = Batch.from_systems([systems[0], bad, systems[2]], gaussian=gaussian, dt=DT)
+    b.run(6)
+    st = b.status()
+    assert st[1] & 0x2, "the NaN replica raises PB_STATUS_NONFINITE"
+    assert st[0] == 0 and st[2] == 0
+    vf = "vd" if gaussian else "v"
+    for k in (0, 2):
+        p = alone_md(systems[k], gaussian)
+        p.run(DT, 6)
+        assert_same(b.get(k, "r"), p.get("r"), f"system {k} positions")
+        assert_same(b.get(k, vf), p.get(vf), f"system {k} velocities")
+    r1 = b.get(1, "r")[:, :3]
+    assert np.isnan(r1[0]).any()
+    if not gaussian:
+        # velocity Verlet: the NaN atom takes part in no pair (its distances
+        # compare false), so the replica's other atoms stay finite; the
+        # Gaussian friction couples every atom and spreads the NaN instead
+        assert np.isfinite(r1[1:]).all()

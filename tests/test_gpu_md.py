@@ -78,10 +78,9 @@ def test_cells_bit_exact_1m(cuda_lib, po):
     s = perturbed(W.config_c2(), 0.1, 7)
     p = md(cuda_lib, s, gaussian=True)
     p.calcBlockID()
-    r4 = p.get("r")
-    assert np.array_equal(p.get("cell_of"), po.bin_cells(r4, s.box, s.rc))
-    pid = p.get("pid")
-    assert np.array_equal(np.sort(pid), np.arange(s.n))
+    # the same checks as at C1: cell of every atom, grid, 27-neighbour table,
+    # per-cell member sets in canonical (z, id) order, sorted positions
+    check_cells(p, s, po)
 
 
 def test_force_c1_vs_oracle_and_reference(cuda_lib, po, golden):

@@ -251,3 +251,100 @@ def test_gr_counts_match_reference_kernel(po, golden):
     L = golden["gr_box"][1] - golden["gr_box"][0]
     g = po.gr_normalise(counts, n, float(L) ** 3, rstep)
     assert g[0] == 0 and g.max() > 1.5  # the perturbed lattice's first shell
+
+
+# ---- velocity initialisation, rescaling and the annealing stage ---------------
+# Golden items 10-12 of tests/golden/make_golden.py: adjustVelocity_F4 /
+# adjustVelocity_VD, scaleTemp (mulArray), the soft-core force of
+# initialAnnealing (MDpairForce<potentialSC>), constTemp's correction
+# (correctConstTemp_F4), the Euler step (calcA_F4 + propagateEuler_F4) and a
+# short initialAnnealing, all from the reference's own kernels.
+
+def _c1_oracle(golden, v=None):
+    r4 = golden["c1_r4"]
+    return po_oracle(golden, r4, v)
+
+
+def po_oracle(golden, r4, v):
+    import pyoracle
+    return pyoracle.Oracle(golden["c1_box"], W.single_type_lj(), 2.5,
+                           r4[:, :3].astype(np.float64),
+                           None if v is None else np.asarray(v, np.float64))
+
+
+def test_adjust_velocities_matches_reference(po, golden):
+    v1 = float(golden["vel_v1_T"][0])
+    O = _c1_oracle(golden, golden["vel_in"])
+    O.adjust_velocities(v1)
+    v = O.get("v")
+    # FP32 velocities of adjustVelocity_F4: (v - mean) * v1 rsqrt(var) in FP64,
+    # rounded once to FP32
+    assert np.abs(v - golden["adjust_vv_v4"][:, :3]).max() <= 4e-7 * np.abs(v).max()
+    # adjustVelocity_VD keeps FP64: agreement to FP64 summation order
+    assert np.abs(v - golden["adjust_gauss_vd"]).max() < 1e-13
+    assert np.abs(v.mean(0)).max() < 1e-12
+    assert np.allclose(v.std(0), v1, rtol=1e-12)
+
+
+def test_scale_temp_matches_reference(po, golden):
+    O = _c1_oracle(golden, golden["vel_in"])
+    f = O.scale_temp(1.1)
+    fvv, fg = golden["scale_factors"]
+    # GaussianThermo::scaleTemp takes T0 from calcTemp() as `real` (FP32), then
+    # an FP64 square root; cudaParticleMD::scaleTemp is FP32 throughout
+    assert f == pytest.approx(fg, rel=1e-7)
+    assert f == pytest.approx(fvv, rel=1e-6)
+    assert np.allclose(O.get("v"), golden["scale_gauss_vd"], rtol=1e-7, atol=1e-9)
+    assert np.allclose(O.get("v"), golden["scale_vv_v4"][:, :3], rtol=1e-6, atol=1e-7)
+
+
+def test_softcore_force_and_euler_match_reference(po, golden):
+    rc, f0, dt = golden["sc_rc_f0_dt"]
+    O = _c1_oracle(golden, golden["c1_v"])
+    O.forces_softcore(rc, f0)
+    F = O.get("F")
+    Fr = golden["sc_F"][:, :3].astype(np.float64)
+    L = float(golden["c1_box"][1])
+    x = golden["c1_r4"][:, :3]
+    interior = np.all((x > 2.5) & (x < L - 2.5), axis=1)
+    # as for the LJ force: FP32 rounding away from the faces, the reference's
+    # minimum image in r^2 near them
+    assert relrms(Fr[interior], F[interior]) < 2e-6
+    assert relrms(Fr, F) < 2e-4
+    assert np.abs(F.sum(0)).max() < 1e-10  # pairwise and antisymmetric
+    lam = O.const_temp()
+    T_ref, lam_ref = golden["sc_consttemp_T_lambda"]
+    assert lam == pytest.approx(lam_ref, rel=1e-4)
+    assert relrms(golden["sc_F_corrected"][:, :3].astype(np.float64), O.get("F")) < 2e-4
+    O.euler(dt)
+    d = O.get("r") - golden["sc_euler_r4"][:, :3]
+    d -= L * np.round(d / L)
+    assert np.abs(d).max() < 1e-5
+    assert np.abs(O.get("v") - golden["sc_euler_v4"][:, :3]).max() < 1e-6
+
+
+def test_softcore_force_is_zero_beyond_its_range(po):
+    box = np.array([0, 10, 0, 10, 0, 10], np.float32)
+    for d, expect in ((0.6, 1.0 * np.cos(0.6 / 1.2 * np.pi / 2)), (1.3, 0.0)):
+        rr = np.full((2, 3), 0.5)
+        rr[1, 0] += d
+        O = po.Oracle(box, W.single_type_lj(), 2.5, rr)
+        O.forces_softcore(1.2, 1.0)
+        F = O.get("F")
+        assert F[0, 0] == pytest.approx(-expect, abs=1e-15)
+        assert F[1, 0] == pytest.approx(expect, abs=1e-15)
+
+
+def test_initial_annealing_matches_reference(po, golden):
+    steps, dt, rc, f0, T = golden["anneal_args"]
+    O = _c1_oracle(golden, golden["c1_v"])
+    O.initial_annealing(int(steps), dt, rc, f0, T)
+    L = float(golden["c1_box"][1])
+    d = O.get("r") - golden["anneal_r4"][:, :3]
+    d -= L * np.round(d / L)
+    assert np.abs(d).max() < 2e-5
+    assert np.abs(O.get("v") - golden["anneal_v4"][:, :3]).max() < 2e-4
+    # the final rescale sets T = 0.72 exactly (up to the (3N - 1) / 3N factor)
+    ke = O.kinetic()
+    n = len(golden["c1_r4"])
+    assert 2 * ke / (3 * n) == pytest.approx(T * (3 * n - 1) / (3 * n), rel=1e-12)

@@ -5,8 +5,9 @@ owns all device memory through its own pool, or a latency-critical loop that
 must not allocate.  pb_cells_build_noalloc serves them with every scratch
 array in one fixed-size static device array.  These tests check it through
 the C ABI against the regular handle-based build (pb_md_build_cells), bit for
-bit, on two calls in a row with different inputs, and check that oversized
-inputs are rejected.  This file is collected last on purpose.
+bit, on two calls in a row with different inputs, with and without a type
+array, that the calls allocate no device memory, and that oversized inputs
+are rejected.  This file is collected last on purpose.
 """
 import ctypes as C
 
@@ -27,13 +28,25 @@ def _perturbed(seed):
     return s
 
 
+def _call(lib, r4, typ, n, s, start, pid, slot, rs):
+    import torch
+    cell6 = np.ascontiguousarray(s.box, np.float32)
+    return lib.pb_cells_build_noalloc(
+        C.c_void_p(r4.data_ptr()), None if typ is None else C.c_void_p(typ.data_ptr()), n,
+        cell6.ctypes.data_as(C.POINTER(C.c_float)), C.c_float(s.rc),
+        C.c_void_p(start.data_ptr()), C.c_void_p(pid.data_ptr()), C.c_void_p(slot.data_ptr()),
+        C.c_void_p(rs.data_ptr()), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+
+
 def test_noalloc_build_matches_handle_build(cuda_lib):
     import torch
     from particlebase_b200.md import from_system
 
     lib = cuda_lib
     dev = torch.device("cuda", 0)
-    for seed in (3, 4):  # two calls in a row; the second reuses the scratch
+    # two calls in a row with a type array (the second reuses the scratch), then
+    # one without: all-zero types come from the scratch array itself
+    for seed, with_types in ((3, True), (4, True), (5, False)):
         s = _perturbed(seed)
         p = from_system(s)
         p.calcBlockID()
@@ -41,19 +54,17 @@ def test_noalloc_build_matches_handle_build(cuda_lib):
         n = s.n
         ncells = len(start_ref) - 1
         r4 = torch.from_numpy(p.get("r")).to(dev)
-        typ = torch.zeros(n, dtype=torch.int16, device=dev)
+        typ = torch.zeros(n, dtype=torch.int16, device=dev) if with_types else None
         start = torch.full((ncells + 1,), -1, dtype=torch.int32, device=dev)
         pid = torch.full((n,), -1, dtype=torch.int32, device=dev)
         slot = torch.full((n,), -1, dtype=torch.int32, device=dev)
-        rs = torch.zeros((n, 4), dtype=torch.float32, device=dev)
-        cell6 = np.ascontiguousarray(s.box, np.float32)
+        rs = torch.full((n, 4), -7.0, dtype=torch.float32, device=dev)
         torch.cuda.synchronize()
-        rc = lib.pb_cells_build_noalloc(
-            C.c_void_p(r4.data_ptr()), C.c_void_p(typ.data_ptr()), n,
-            cell6.ctypes.data_as(C.POINTER(C.c_float)), C.c_float(s.rc),
-            C.c_void_p(start.data_ptr()), C.c_void_p(pid.data_ptr()), C.c_void_p(slot.data_ptr()),
-            C.c_void_p(rs.data_ptr()), C.c_void_p(torch.cuda.current_stream().cuda_stream))
-        assert rc == 0
+        free0 = torch.cuda.mem_get_info()[0]
+        assert _call(lib, r4, typ, n, s, start, pid, slot, rs) == 0
+        torch.cuda.synchronize()
+        if seed == 4:  # the same kernels as the first call: loaded, scratch resolved
+            assert torch.cuda.mem_get_info()[0] == free0, "the call allocated device memory"
         assert np.array_equal(start.cpu().numpy().view(np.uint32), start_ref)
         got_pid = pid.cpu().numpy().view(np.uint32)
         assert np.array_equal(got_pid, pid_ref)
@@ -61,6 +72,8 @@ def test_noalloc_build_matches_handle_build(cuda_lib):
         slot_ref[pid_ref] = np.arange(n, dtype=np.uint32)
         assert np.array_equal(slot.cpu().numpy().view(np.uint32), slot_ref)
         assert np.array_equal(rs.cpu().numpy().view(np.uint32), rs_ref.view(np.uint32))
+        if not with_types:
+            assert np.all(rs.cpu().numpy()[:, 3].view(np.int32) == 0)
         p.close()
 
 
