@@ -200,12 +200,12 @@ def run_reference_arm(args) -> dict:
         po.build(ref=True)
     except Exception:
         pass
-    s = W.config_c2()
-    steps = max(1, min(args.steps, 8))
+    s = W.config_c2(seed=2)  # the system rank 0 of the GPU arm times
+    steps = max(1, args.steps)
     if po.ref_available():
         R = po.RefKernels(s.box, s.rc, s.r, s.v, s.mass, s.types, [1.0, 1.0], gaussian=True)
-        for _ in range(max(1, min(args.warmup, 2))):
-            R.run(DT, 1)  # includes the first (from-scratch) sort
+        for _ in range(max(1, args.warmup)):
+            R.run(DT, 1)  # the first includes the from-scratch sort
         t = time.perf_counter()
         rc = R.run(DT, steps)
         el = time.perf_counter() - t
@@ -215,7 +215,7 @@ def run_reference_arm(args) -> dict:
                   f"one-thread blocks run in parallel by OpenMP; NR rc={rc}")
     else:
         O = po.Oracle(s.box, s.lj, s.rc, s.r, s.v)
-        O.run(1, DT, mode="gauss")
+        O.run(max(1, args.warmup), DT, mode="gauss")
         t = time.perf_counter()
         O.run(steps, DT, mode="gauss")
         el = time.perf_counter() - t
@@ -584,10 +584,10 @@ def main(argv=None) -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="all", choices=["all", "c2", "c3", "c4", "c5"],
                     help="c2: 1M-atom single system; c3: batched replicas; c4: served jobs; "
-                         "all: the c2 line with c3 under 'batched' and a c4 sample under "
-                         "'served'")
-    ap.add_argument("--jobs", type=int, default=None,
-                    help="served jobs (default: 2000 with --workload c4, 200 in 'all')")
+                         "all: the c2 line with c3 under 'batched', c4 under 'served' and "
+                         "c5 under 'kob_andersen'")
+    ap.add_argument("--jobs", type=int, default=2000,
+                    help="served jobs of the C4 stream (default: all 2,000)")
     ap.add_argument("--chunk-ms", type=float, default=50.0)
     ap.add_argument("--ka-atoms", type=int, default=8_388_608)
     ap.add_argument("--ka-steps", type=int, default=300)
@@ -606,7 +606,7 @@ def main(argv=None) -> int:
     try:
         if args.workload in ("c3", "c4", "c5"):
             out = {"c3": lambda: run_batched(args, dist),
-                   "c4": lambda: run_served(args, dist, args.jobs or 2000),
+                   "c4": lambda: run_served(args, dist, args.jobs),
                    "c5": lambda: run_kob_andersen(args, dist)}[args.workload]()
             if dist.rank == 0:
                 print(json.dumps(out), flush=True)
@@ -614,7 +614,7 @@ def main(argv=None) -> int:
         out = run_ours(args, dist)
         if args.workload == "all":
             out["batched"] = run_batched(args, dist)
-            out["served"] = run_served(args, dist, args.jobs or 200)
+            out["served"] = run_served(args, dist, args.jobs)
             out["kob_andersen"] = run_kob_andersen(args, dist)
         if dist.rank == 0:
             if dist.ws == 1 and not args.no_cpu_baseline:

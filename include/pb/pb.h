@@ -59,6 +59,10 @@ typedef struct pb_md pb_md;
 /* Creation flags */
 #define PB_MD_VEL_FP64 0x1u   /* keep velocities in FP64 planes (GaussianThermo::vd) */
 #define PB_MD_ACC_FP64 0x2u   /* accumulate per-atom force sums in FP64 */
+#define PB_MD_HALF_SHELL 0x4u /* evaluate every unordered pair once (Newton's third law)
+                                 with exact fixed-point force sums, instead of every ordered
+                                 pair as calcF_IJpairWithBlock_F4 does (the default);
+                                 ignored with PB_MD_ACC_FP64 */
 
 /* Fields for pb_md_get / pb_md_set */
 typedef enum pb_field {
@@ -145,6 +149,14 @@ int pb_md_build_cells(pb_md *h);
  * also accumulates PE, shifted PE and virial (FP64) for pb_md_reduce. */
 #define PB_FORCE_ENERGY 0x1u
 int pb_md_force(pb_md *h, uint32_t flags);
+/* Failure-detection test hook (no counterpart in the reference): one force
+ * call in which the force kernel's producer warps withhold
+ * their first hand-off to the consumer warps, with every hand-off wait bounded
+ * by `polls` polls of at most 1 us.  The consumers' wait runs out, the CTAs
+ * end early, the call returns PB_OK and the status word carries
+ * PB_STATUS_WAIT_TIMEOUT; the forces of that call are not meaningful.  The
+ * handle stays usable: the next pb_md_force is complete again. */
+int pb_md_force_wait_test(pb_md *h, uint32_t polls);
 /* cudaParticleVV::clearForce (cudaParticleVV.cu:10-15): F = Fold = 0. */
 int pb_md_clear_force(pb_md *h);
 /* cudaParticleVV::TimeEvolution (cudaParticleVV.cu:17-34). */
@@ -265,11 +277,15 @@ int pb_peak_fp32(double *tflops);
  * Device pointers: r4 (float4[n] positions), type (uint16[n] or NULL for all
  * zero); outputs start (uint32[C+1], C from pb_plan_grid, cells in the key
  * order of pb_plan_columns, z fastest), pid (uint32[n]), slot (uint32[n]),
- * rs4 (float4[n] sorted positions, w = type bits).  Runs on `stream` (a
- * cudaStream_t, NULL = legacy default) and returns after it has finished.
- * The first call on a device resolves the static array's device address; make
- * that first call before any stream capture.  All calls share the one array:
- * calls that overlap on the GPU race, so serialise them. */
+ * rs4 (float4[n] sorted positions, w = type bits).  Enqueued on `stream` (a
+ * cudaStream_t, NULL = legacy default) without waiting for it: the outputs
+ * are ready when the stream reaches this point, and no host memory of the
+ * call is read after it returns.  The first call on a device resolves the
+ * static array's device address and keeps it for later calls; make that first
+ * call before any stream capture, use one context per device (the CUDA
+ * runtime's primary context) and do not reset the device between calls.  All
+ * calls share the one array: calls that overlap on the GPU race, so serialise
+ * them. */
 int pb_cells_build_noalloc(const void *r4, const uint16_t *type, uint32_t n, const float cell6[6],
                            float rmax, uint32_t *start, uint32_t *pid, uint32_t *slot, void *rs4,
                            void *stream);

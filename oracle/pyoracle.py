@@ -21,7 +21,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_ORACLE = os.path.join(HERE, "liboracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "libpbref.so")
-REFERENCE_DIR = os.environ.get("PB_REFERENCE_DIR", "/root/reference")
+# the reference checkout: PB_REFERENCE_DIR, else a `reference` directory beside
+# this repository
+REFERENCE_DIR = os.environ.get(
+    "PB_REFERENCE_DIR", os.path.normpath(os.path.join(HERE, os.pardir, os.pardir, "reference")))
 
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")

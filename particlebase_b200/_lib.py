@@ -25,6 +25,7 @@ FIELD = {
 
 VEL_FP64 = 0x1
 ACC_FP64 = 0x2
+HALF_SHELL = 0x4
 FORCE_ENERGY = 0x1
 MODE_VV = 0
 MODE_GAUSS = 1
@@ -117,6 +118,7 @@ def _declare(L: C.CDLL) -> None:
         "pb_md_minimize": [vp, u32, f32, f32],
         "pb_md_force_softcore": [vp, f32, f32],
         "pb_md_step_euler": [vp, f32],
+        "pb_md_force_wait_test": [vp, u32],
         "pb_md_get": [vp, i32, vp, C.c_size_t],
         "pb_md_set": [vp, i32, vp, C.c_size_t],
         "pb_md_field_bytes": [vp, i32, C.POINTER(C.c_size_t)],

@@ -31,13 +31,14 @@ class Batch:
 
     def __init__(self, natoms: Sequence[int], gaussian: bool = False,
                  fp64_velocities: bool | None = None, fp64_forces: bool = False,
-                 _handle: C.c_void_p | None = None):
+                 _handle: C.c_void_p | None = None, half_shell: bool = False):
         self.lib = L.lib()
         self.gaussian = bool(gaussian)
         if fp64_velocities is None:
             fp64_velocities = self.gaussian
         self.fp64_velocities = bool(fp64_velocities)
-        self.flags = (L.VEL_FP64 if fp64_velocities else 0) | (L.ACC_FP64 if fp64_forces else 0)
+        self.flags = ((L.VEL_FP64 if fp64_velocities else 0) | (L.ACC_FP64 if fp64_forces else 0) |
+                      (L.HALF_SHELL if half_shell else 0))
         if _handle is None:
             n = np.ascontiguousarray(np.asarray(natoms, np.uint32))
             h = C.c_void_p()
@@ -126,8 +127,10 @@ class Batch:
     @classmethod
     def from_systems(cls, systems: Sequence[LJSystem], gaussian: bool = False, dt: float = 0.005,
                      fp64_velocities: bool | None = None, fp64_forces: bool = False,
-                     tuning: tuple[int, float] | None = None) -> "Batch":
-        b = cls([s.n for s in systems], gaussian, fp64_velocities, fp64_forces)
+                     tuning: tuple[int, float] | None = None,
+                     half_shell: bool = False) -> "Batch":
+        b = cls([s.n for s in systems], gaussian, fp64_velocities, fp64_forces,
+                half_shell=half_shell)
         dts = np.broadcast_to(np.asarray(dt, np.float64), (len(systems),))
         for k, s in enumerate(systems):
             b.add_system(k, s, float(dts[k]))
@@ -150,7 +153,7 @@ class Batch:
         self._ck(self.lib.pb_batch_repack(self.h, _fptr(src_a), _fptr(nat), len(src_a),
                                           C.byref(h)), "repack")
         out = Batch(nat, self.gaussian, self.fp64_velocities, bool(self.flags & L.ACC_FP64),
-                    _handle=h)
+                    _handle=h, half_shell=bool(self.flags & L.HALF_SHELL))
         for k, s in enumerate(src_a):
             if s >= 0:
                 out.kB[k] = self.kB[s]

@@ -116,7 +116,10 @@ MD_DRIVERS = ("testMD1", "testMD2", "testMD3", "testMD4", "testMD4n", "calcgr1")
 
 
 def reference_dir() -> str:
-    return os.environ.get("PB_REFERENCE_DIR", "/root/reference")
+    """The reference checkout: PB_REFERENCE_DIR, else a `reference` directory
+    beside this repository."""
+    return os.environ.get("PB_REFERENCE_DIR",
+                          os.path.normpath(os.path.join(ROOT, os.pardir, "reference")))
 
 
 def build_drivers(names=MD_DRIVERS, ref_dir: str | None = None, force: bool = False) -> list[str]:

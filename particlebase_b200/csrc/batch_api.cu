@@ -401,9 +401,9 @@ int pb_batch_estimate_bytes(const uint32_t *natoms, const float *cells6, const f
   if (!natoms || !cells6 || !rmax || !bytes || nsys == 0) return PB_ERR_ARG;
   // per atom: r, F[2], rs (16 B each), minv, mass, key, within, pid_tmp, pid,
   // slot (4 B each), x, y, z, type mirrors of rs (16 B), type (2 B),
-  // velocities (16 or 24 B), sysid (4 B)
+  // velocities (16 or 24 B), sysid (4 B), fixed-point force sums (48 B)
   const size_t per_atom = 16 * 4 + 4 * 7 + 16 + 2 + ((flags & PB_MD_VEL_FP64) ? 24 : 16) +
-                          (nsys > 1 ? 4 : 0);
+                          (nsys > 1 ? 4 : 0) + 48;
   size_t total = 0;
   for (uint32_t s = 0; s < nsys; ++s) {
     Grid g;

@@ -254,7 +254,8 @@ int engine_init(Engine &e, const uint32_t *natoms, uint32_t nsys, uint32_t flags
             dalloc(e, &e.d_sysint, nsys) == cudaSuccess && dalloc(e, &e.d_map, e.nblocks) == cudaSuccess &&
             dalloc(e, &e.ipartials, (size_t)8 * e.nblocks) == cudaSuccess &&
             dalloc(e, &e.sc, nsys) == cudaSuccess && dalloc(e, &e.status, nsys) == cudaSuccess &&
-            dalloc(e, &e.d_fac, nsys) == cudaSuccess && dalloc(e, &e.d_lj, nsys) == cudaSuccess;
+            dalloc(e, &e.d_fac, nsys) == cudaSuccess && dalloc(e, &e.d_lj, nsys) == cudaSuccess &&
+            dalloc(e, &e.facc, (size_t)6 * N) == cudaSuccess;
   if (flags & PB_MD_VEL_FP64)
     ok = ok && dalloc(e, &e.vd, (size_t)3 * N) == cudaSuccess;
   else
@@ -267,6 +268,7 @@ int engine_init(Engine &e, const uint32_t *natoms, uint32_t nsys, uint32_t flags
   if (e.v) E_CUDA(cudaMemsetAsync(e.v, 0, sizeof(float4) * N, e.stream));
   if (e.vd) E_CUDA(cudaMemsetAsync(e.vd, 0, sizeof(double) * 3 * N, e.stream));
   E_CUDA(cudaMemsetAsync(e.type, 0, sizeof(uint16_t) * N, e.stream));
+  E_CUDA(cudaMemsetAsync(e.facc, 0, sizeof(unsigned long long) * 6 * N, e.stream));
   E_CUDA(cudaMemsetAsync(e.sc, 0, sizeof(DevScalars) * nsys, e.stream));
   E_CUDA(cudaMemsetAsync(e.status, 0, sizeof(uint32_t) * nsys, e.stream));
   E_CUDA(cudaMemcpyAsync(e.d_map, map.data(), sizeof(BlockMap) * e.nblocks, cudaMemcpyHostToDevice,
@@ -298,6 +300,7 @@ void engine_free(Engine &e) {
   dfree(e, e.sc);
   dfree(e, e.status);
   dfree(e, e.d_fac);
+  dfree(e, e.facc);
   dfree(e, e.d_lj);
   dfree(e, e.steps_left);
   free_nlist(e);
@@ -470,6 +473,7 @@ int engine_setup_cells(Engine &e) {
   uint64_t ncells = 0;
   uint32_t mirror = 0;
   e.cap_max = 0;
+  e.cap_half_max = 0;
   // grids and plans first, so that the item and column arrays are sized once
   std::vector<std::shared_ptr<const Plan>> plans(e.nsys);
   size_t nitem_all = 0, ncol_all = 0;
@@ -483,7 +487,9 @@ int engine_setup_cells(Engine &e) {
     const double apc = (double)P.n / g.ncells;
     P.seg = choose_segment(apc, g.n[2], e.seg_scale, P.lj_set ? P.lj.nt : 1);
     P.cap = (uint32_t)choose_capacity(apc, P.seg);
+    P.cap_half = (uint32_t)choose_capacity_half(apc, P.seg);
     e.cap_max = std::max(e.cap_max, P.cap);
+    e.cap_half_max = std::max(e.cap_half_max, P.cap_half);
     plans[s] = cached_plan(g, P.seg);
     nitem_all += plans[s]->items.size();
     ncol_all += plans[s]->rank.size();
@@ -527,6 +533,7 @@ int engine_setup_cells(Engine &e) {
     D.lj = s;
     D.dt = P.dt;
     D.cap = P.cap;
+    D.cap_half = P.cap_half;
     D.mirror0 = mirror;
     mirror += (P.n + 3u) & ~3u;
     rank_all.insert(rank_all.end(), rank.begin(), rank.end());
@@ -652,6 +659,14 @@ ForceBufs engine_fbufs(Engine &e) {
   b.queue = e.fqueue;
   b.status = e.status;
   b.steps_left = e.steps_left;
+  b.facc = e.facc;
+  b.fbig = e.facc + (size_t)3 * e.N;
+  b.nacc = e.N;
+  b.cap_half = (int)e.cap_half_max;
+  b.map = e.d_map;
+  b.nblocks = e.nblocks;
+  b.wait_polls = e.force_wait_polls;
+  b.test_flags = e.force_test_flags;
   return b;
 }
 
@@ -798,8 +813,12 @@ int engine_force(Engine &e, bool energy) {
     e.energy_valid = energy;
     return PB_OK;
   }
-  cudaError_t c = launch_force(engine_fbufs(e), nt, energy, (e.flags & PB_MD_ACC_FP64) != 0,
-                               e.force_threads, e.stream);
+  // every ordered pair (the reference's full shell), or with PB_MD_HALF_SHELL
+  // every unordered pair once with exact fixed-point sums
+  const bool full = (e.flags & PB_MD_ACC_FP64) != 0 || (e.flags & PB_MD_HALF_SHELL) == 0;
+  cudaError_t c = full ? launch_force(engine_fbufs(e), nt, energy, (e.flags & PB_MD_ACC_FP64) != 0,
+                                      e.force_threads, e.stream)
+                       : launch_force_half(engine_fbufs(e), nt, energy, e.stream);
   if (c != cudaSuccess) return cuda_fail(e, c, "force");
   e.last = e.cur;
   if (energy) {

@@ -22,6 +22,7 @@ struct SysParams {
   Grid grid{};
   int seg = 1;
   uint32_t cap = 0;
+  uint32_t cap_half = 0;  // stage capacity of the half-shell force kernel
   double m0 = 1.0;
   float dt = 0.005f;
   std::vector<uint32_t> key_of_ref, ref_of_key;  // reference cell id <-> packed key - cell0
@@ -75,6 +76,10 @@ struct Engine {
   double *fpartials = nullptr;
   uint32_t *fqueue = nullptr;  // the force kernel's item counter
   uint32_t cap_max = 0;
+  uint32_t cap_half_max = 0;
+  unsigned long long *facc = nullptr;  // half-shell force sums: fine and coarse, 2 x 3 x N
+  uint32_t force_test_flags = 0;       // ForceBufs::test_flags of the next force call
+  uint32_t force_wait_polls = 0;       // ForceBufs::wait_polls of the next force call
   bool energy_valid = false;
   bool mv2_fresh = false;  // sc.mv2 holds sum m v^2 of the current velocities
 

@@ -779,6 +779,7 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
     return p;
   };
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t polls = b.wait_polls ? b.wait_polls : kWaitPolls;
   if (threadIdx.x == 0) {
     for (int k = 0; k < 2; ++k) {
       mbar_init(&full[k], 1);
@@ -796,7 +797,7 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
     // outcome through its barrier), then stage the next item into it
     auto wait_empty = [&](int bf, uint32_t parity) -> bool {
       if (threadIdx.x == 0) {
-        const bool ok = mbar_wait_or_abort(&empty[bf], parity, &kNeverAbort);
+        const bool ok = mbar_wait_or_abort(&empty[bf], parity, &kNeverAbort, polls);
         wait_ok = ok;
         if (!ok) {
           atomicOr(&b.status[desc[bf].sys], kStatusWaitTimeout);
@@ -854,7 +855,10 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
         if (threadIdx.x == 0) abort_flag = 1;
         return;
       }
-      if (threadIdx.x == 0) mbar_arrive(&full[bf]);
+      // test hook (failure-detection test entry only): withhold the first
+      // hand-off so that the consumers' bounded wait runs out
+      const bool withhold = (b.test_flags & 1u) && n == 0;
+      if (threadIdx.x == 0 && !withhold) mbar_arrive(&full[bf]);
     }
     // the last item: wait for the consumers, then its energy partials
     if (n >= 1) {
@@ -873,7 +877,7 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
   uint16_t *tb = mylist + 32 * kListLen;
   for (uint32_t n = 0;; ++n) {
     const int bf = n & 1;
-    bool ok = lane != 0 || mbar_wait_or_abort(&full[bf], (n >> 1) & 1u, abort_v);
+    bool ok = lane != 0 || mbar_wait_or_abort(&full[bf], (n >> 1) & 1u, abort_v, polls);
     ok = __shfl_sync(0xffffffffu, ok, 0);
     if (!ok) {
       if (lane == 0 && !*abort_v) atomicOr(&b.status[0], kStatusWaitTimeout);

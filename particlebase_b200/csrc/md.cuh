@@ -25,6 +25,8 @@
 
 namespace pb {
 
+struct BlockMap;  // integrate.cuh
+
 // One periodic system inside the packed arrays.
 struct SysDesc {
   Grid g;
@@ -36,6 +38,7 @@ struct SysDesc {
   float dt;                 // time step
   uint32_t cap;             // staged-atom capacity of this system's force CTAs
   uint32_t mirror0;         // first slot of this system in the SoA mirrors (multiple of 4)
+  uint32_t cap_half;        // staged-atom capacity of the half-shell force CTAs
 };
 
 // Work item of the force kernel: one (x, y) column of one system, z cells
@@ -90,6 +93,16 @@ struct ForceBufs {
   float sc_rc, sc_f0;          // soft-core force law: range and strength
   uint32_t *queue;           // [0] next unclaimed item, [1] CTAs done claiming; zero
                              // between launches (the last CTA resets them)
+  // half-shell kernel (force_half.cu)
+  unsigned long long *facc;  // fixed-point force sums (2^-32 units), planes x, y, z of
+                             // nacc entries indexed by sorted slot; zero between calls
+  unsigned long long *fbig;  // the same in units of 1/2, for shares of 2^22 and more
+  uint32_t nacc;             // atoms of all systems
+  int cap_half;              // stage capacity of the launch (max over systems)
+  const BlockMap *map;       // integration blocks (per-system atom ranges)
+  uint32_t nblocks;
+  uint32_t wait_polls;       // bound of the hand-off waits, 0 = default
+  uint32_t test_flags;       // bit 0: withhold the first hand-off (failure-detection test)
 };
 
 // Verlet neighbour list of one system: row s holds the build-time sorted
@@ -118,6 +131,9 @@ struct NlistBufs {
 cudaError_t launch_cell_build(const CellBufs &b, cudaStream_t s);
 cudaError_t launch_force(const ForceBufs &b, int nt_max, bool energy, bool acc64,
                          int block_threads, cudaStream_t s);
+// Half-shell force (each pair once, fixed-point sums) followed by the
+// conversion of the sums to F; FP32 pair arithmetic.
+cudaError_t launch_force_half(const ForceBufs &b, int nt_max, bool energy, cudaStream_t s);
 // Relaxation force for steepest descent: pair distance floored at sigma/2.
 cudaError_t launch_force_capped(const ForceBufs &b, int nt_max, cudaStream_t s);
 // Soft-core force f0 cos(pi r / 2 sc_rc) along r (potentialSC), for annealing.

@@ -207,6 +207,17 @@ int pb_md_force(pb_md *h, uint32_t flags) {
   return h ? engine_force(h->e, (flags & PB_FORCE_ENERGY) != 0) : PB_ERR_ARG;
 }
 
+int pb_md_force_wait_test(pb_md *h, uint32_t polls) {
+  if (!h || polls == 0) return PB_ERR_ARG;
+  h->e.force_test_flags = 1u;
+  h->e.force_wait_polls = polls;
+  const int rc = engine_force(h->e, false);
+  h->e.force_test_flags = 0u;
+  h->e.force_wait_polls = 0u;
+  if (rc) return rc;
+  return cudaStreamSynchronize(h->e.stream) == cudaSuccess ? PB_OK : PB_ERR_CUDA;
+}
+
 int pb_md_clear_force(pb_md *h) { return h ? engine_clear_force(h->e) : PB_ERR_ARG; }
 
 int pb_md_step_vv(pb_md *h, float dt) {

@@ -81,7 +81,9 @@ int choose_segment(double atoms_per_cell, int nz, double scale, int nt) {
   if (const char *e = env_once(0)) seg = std::atoi(e);
   seg = std::max(1, std::min(seg, force_max_segment()));
   seg = std::min(seg, nz);
-  while (seg > 1 && force_smem_per_cta(choose_capacity(apc, seg), nt) > 112 * 1024) --seg;
+  while (seg > 1 && (force_smem_per_cta(choose_capacity(apc, seg), nt) > 112 * 1024 ||
+                     force_half_smem_per_cta(choose_capacity_half(apc, seg), nt) > 112 * 1024))
+    --seg;
   return seg;
 }
 
@@ -92,6 +94,15 @@ int choose_capacity(double atoms_per_cell, int seg) {
   const double cap = factor * expect + 128.0;
   // the largest launch shape (8 warps, 8 types) bounds every launch's memory
   static const double max_atoms = (double)force_max_capacity(8, kMaxTypes);
+  return (int)std::min(cap, max_atoms);
+}
+
+int choose_capacity_half(double atoms_per_cell, int seg) {
+  const double expect = 5.0 * (seg + 2) * std::max(atoms_per_cell, 1.0);
+  double factor = 1.15;
+  if (const char *e = env_once(1)) factor = std::atof(e);
+  const double cap = factor * expect + 128.0;
+  static const double max_atoms = (double)force_half_max_capacity(kMaxTypes);
   return (int)std::min(cap, max_atoms);
 }
 

@@ -32,6 +32,8 @@ int choose_segment(double atoms_per_cell, int nz, double scale = 1.0, int nt = 1
 // Shared-memory capacity (atoms) of a force CTA staging 9 columns x (seg + 2)
 // cells at the given mean occupancy, with headroom for fluctuations.
 int choose_capacity(double atoms_per_cell, int seg);
+// The same for the half-shell force kernel, which stages 5 columns.
+int choose_capacity_half(double atoms_per_cell, int seg);
 
 // Force work items of one system whose packed cell keys start at cell0, with
 // the column ranking `rank` (reference column -> rank) and its inverse `xy`.
@@ -45,5 +47,8 @@ int force_max_capacity(int warps, int nt);
 // Shared memory (dynamic plus an upper bound of the static part) of one
 // default-shape force CTA with staged-atom capacity `cap` and `nt` types.
 int force_smem_per_cta(int cap, int nt);
+// The same two for the half-shell force kernel (force_half.cu).
+int force_half_max_capacity(int nt);
+int force_half_smem_per_cta(int cap, int nt);
 
 }  // namespace pb

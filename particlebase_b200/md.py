@@ -33,13 +33,14 @@ class MDSystem:
     """One periodic LJ system resident on the GPU (a pb_md handle)."""
 
     def __init__(self, n: int, gaussian: bool = False, fp64_velocities: bool | None = None,
-                 fp64_forces: bool = False):
+                 fp64_forces: bool = False, half_shell: bool = False):
         self.lib = L.lib()
         self.n = int(n)
         self.gaussian = bool(gaussian)
         if fp64_velocities is None:
             fp64_velocities = self.gaussian  # GaussianThermo keeps FP64 velocities (vd)
-        flags = (L.VEL_FP64 if fp64_velocities else 0) | (L.ACC_FP64 if fp64_forces else 0)
+        flags = ((L.VEL_FP64 if fp64_velocities else 0) | (L.ACC_FP64 if fp64_forces else 0) |
+                 (L.HALF_SHELL if half_shell else 0))
         self.fp64_velocities = bool(fp64_velocities)
         h = C.c_void_p()
         L.check(self.lib.pb_md_create(self.n, flags, C.byref(h)), "pb_md_create")
@@ -176,6 +177,12 @@ class MDSystem:
         self._ck(self.lib.pb_md_gr(self.h, C.c_float(rstep), C.c_float(rmax),
                                    out.ctypes.data_as(C.c_void_p), C.byref(n)), "gr")
         return out
+
+    def force_wait_test(self, polls: int = 2000) -> None:
+        """Failure-detection test hook: one force call whose hand-off wait is
+        made to run out (pb_md_force_wait_test); raises nothing, sets
+        PB_STATUS_WAIT_TIMEOUT in the status word."""
+        self._ck(self.lib.pb_md_force_wait_test(self.h, int(polls)), "force_wait_test")
 
     def clearForce(self) -> None:
         self._ck(self.lib.pb_md_clear_force(self.h), "clear_force")
@@ -357,11 +364,13 @@ class MDSystem:
 
 def from_system(s: LJSystem, gaussian: bool = False, fp64_velocities: bool | None = None,
                 fp64_forces: bool = False, per_pair_cutoff: bool | None = None,
-                cell_rmax: float | None = None) -> MDSystem:
+                cell_rmax: float | None = None, half_shell: bool = False) -> MDSystem:
     """Build a ready-to-step MDSystem from a host LJSystem (reduced units).
     Cells are at least `cell_rmax` wide (default: the cutoff; a neighbour list
-    needs cutoff + thickness)."""
-    p = MDSystem(s.n, gaussian=gaussian, fp64_velocities=fp64_velocities, fp64_forces=fp64_forces)
+    needs cutoff + thickness).  half_shell: evaluate every unordered pair once
+    (Newton's third law, fixed-point sums) instead of every ordered pair."""
+    p = MDSystem(s.n, gaussian=gaussian, fp64_velocities=fp64_velocities, fp64_forces=fp64_forces,
+                 half_shell=half_shell)
     p.setCell(s.box)
     p.kB = 1.0
     p.rmax2 = float(s.rc) ** 2

@@ -66,6 +66,16 @@ def nve_drift(p, steps=1000):
     return float(np.polyfit(np.arange(len(e)), e, 1)[0] * 1000), float(e.std())
 
 
+def oracle_drift(po, s, steps=1000):
+    """The FP64 oracle's NVE drift on the same start, same definition: energy
+    per atom at t_k from the force evaluation at r(t_k) and v(t_k), steps
+    1..steps fitted (orc_run records both)."""
+    O = po.Oracle(s.box, s.lj, s.rc, s.r, s.v, s.mass, s.types)
+    e = O.run(steps + 1, DT, record=True)
+    tot = (e[1:, 0] + e[1:, 2]) / s.n
+    return float(np.polyfit(np.arange(len(tot)), tot, 1)[0] * 1000)
+
+
 def record(name, **kw):
     RESULTS[name] = kw
     out = os.environ.get("PB_ACCURACY_OUT")
@@ -74,10 +84,13 @@ def record(name, **kw):
             json.dump(RESULTS, fh, indent=1)
 
 
-def check(name, forces, drift, spread):
-    record(name, force_relrms=forces, nve_drift_per_1000=drift, energy_std=spread)
+def check(name, forces, drift, spread, odrift=None):
+    record(name, force_relrms=forces, nve_drift_per_1000=drift, energy_std=spread,
+           oracle_nve_drift_per_1000=odrift)
     assert forces["fp32_acc"] < FORCE_RELRMS and forces["fp64_acc"] < FORCE_RELRMS, forces
     assert abs(drift) < DRIFT, drift
+    if odrift is not None:
+        assert abs(odrift) < DRIFT, odrift
 
 
 def test_accuracy_c1(cuda_lib, po):
@@ -85,7 +98,7 @@ def test_accuracy_c1(cuda_lib, po):
     s = W.config_c1()
     forces = force_errors(po, perturbed(W.config_c1(), seed=11))
     drift, spread = nve_drift(from_system(s))
-    check("C1 fcc 4,000", forces, drift, spread)
+    check("C1 fcc 4,000", forces, drift, spread, oracle_drift(po, W.config_c1()))
 
 
 def test_accuracy_c2(cuda_lib, po):
@@ -120,7 +133,12 @@ def test_accuracy_c3_replicas(cuda_lib, po):
         f = force_errors(po, perturbed(W.uneven_replicas(256, seed=3)[32 * k], seed=20 + k))
         worst = {m: max(worst[m], f[m]) for m in worst}
     drifts, spread = _batch_drift(systems)
-    check("C3 uneven replicas (8 of 256, batched)", worst, max(drifts, key=abs), spread)
+    # the oracle's drift on the first of them, from the same start
+    check("C3 uneven replicas (8 of 256, batched)", worst, max(drifts, key=abs), spread,
+          oracle_drift(po, W.uneven_replicas(256, seed=3)[0]))
+    record("C3 replica 0 (GPU in the batch vs FP64 oracle)", nve_drift_per_1000=drifts[0],
+           oracle_nve_drift_per_1000=RESULTS["C3 uneven replicas (8 of 256, batched)"][
+               "oracle_nve_drift_per_1000"], atoms=systems[0].n)
 
 
 def test_accuracy_c4_jobs(cuda_lib, po):
@@ -131,7 +149,11 @@ def test_accuracy_c4_jobs(cuda_lib, po):
         f = force_errors(po, perturbed(sp.system(), seed=30 + k))
         worst = {m: max(worst[m], f[m]) for m in worst}
     drifts, spread = _batch_drift(systems)
-    check("C4 served jobs (4 of the stream, batched)", worst, max(drifts, key=abs), spread)
+    check("C4 served jobs (4 of the stream, batched)", worst, max(drifts, key=abs), spread,
+          oracle_drift(po, specs[0].system()))
+    record("C4 job 0 (GPU in the batch vs FP64 oracle)", nve_drift_per_1000=drifts[0],
+           oracle_nve_drift_per_1000=RESULTS["C4 served jobs (4 of the stream, batched)"][
+               "oracle_nve_drift_per_1000"], atoms=systems[0].n)
 
 
 @pytest.mark.slow

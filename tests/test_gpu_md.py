@@ -399,3 +399,21 @@ def test_runs_of_odd_length_match_one_run(cuda_lib, gaussian):
     b.run(0.005, 10)
     assert np.array_equal(a.get("r"), b.get("r"))
     assert np.array_equal(a.get("F"), b.get("F"))
+
+
+def test_wait_timeout_is_reported_and_the_handle_recovers(cuda_lib, po):
+    """Failure detection without a GPU fault: a test hook makes the force
+    kernel's producer warps withhold their first hand-off, so the consumer
+    warps' bounded wait (2,000 polls of at most 1 us) runs out.  The call
+    returns, PB_STATUS_WAIT_TIMEOUT is set, and the next force call on the
+    same handle is complete and correct."""
+    s = perturbed(W.config_c1(), 0.05, 3)
+    p = md(cuda_lib, s)
+    p.calcBlockID()
+    assert p.status() == 0
+    p.force_wait_test(2000)
+    assert p.status() & 0x4, "PB_STATUS_WAIT_TIMEOUT"
+    p.calcForce()
+    assert p.status() == 0
+    Fo, _ = oracle_forces(po, s, p.get("r"))
+    assert relrms(p.get("F")[:, :3].astype(np.float64), Fo) < FORCE_RELRMS
