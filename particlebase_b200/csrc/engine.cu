@@ -485,7 +485,8 @@ int engine_setup_cells(Engine &e) {
       return fail(e, PB_ERR_ARG, "cell grid needs at least 3 cells per axis (blocknum > 2)");
     P.grid = g;
     const double apc = (double)P.n / g.ncells;
-    P.seg = choose_segment(apc, g.n[2], e.seg_scale, P.lj_set ? P.lj.nt : 1);
+    const bool half = (e.flags & PB_MD_HALF_SHELL) && !(e.flags & PB_MD_ACC_FP64);
+    P.seg = choose_segment(apc, g.n[2], e.seg_scale, P.lj_set ? P.lj.nt : 1, half);
     P.cap = (uint32_t)choose_capacity(apc, P.seg);
     P.cap_half = (uint32_t)choose_capacity_half(apc, P.seg);
     e.cap_max = std::max(e.cap_max, P.cap);

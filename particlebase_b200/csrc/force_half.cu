@@ -610,10 +610,9 @@ __device__ __forceinline__ void consume_cluster3(const ForceBufs &b, const ItemD
     const uint2 qq = *reinterpret_cast<const uint2 *>(tb + u0 + 4 * q);
     const uint32_t quads[4] = {qq.x & 0xffffu, qq.x >> 16, qq.y & 0xffffu, qq.y >> 16};
     const uint32_t nsteps = min((Q - u0 + 3u) >> 2, (uint32_t)(kChunk / 4));
-#pragma unroll
-    for (int kk = 0; kk < kChunk / 4; ++kk) {
-      if ((uint32_t)kk >= nsteps) break;
-      const uint32_t quad = quads[kk];
+    // one quad: 4 candidate tests, appended through offsets that depend on
+    // the hit bits only, so the list pointer carries one add per quad
+    auto test_quad = [&](uint32_t quad) {
       const float4 x4 = lds_f4(xa + quad * 16u), y4 = lds_f4(ya + quad * 16u),
                    z4 = lds_f4(za + quad * 16u);
       const float2 dxa = __ffma2_rn(make_float2(x4.x, x4.y), m1, xi2);
@@ -624,15 +623,27 @@ __device__ __forceinline__ void consume_cluster3(const ForceBufs &b, const ItemD
       const float2 dzb = __ffma2_rn(make_float2(z4.z, z4.w), m1, zi2);
       const float2 da = __ffma2_rn(dza, dza, __ffma2_rn(dya, dya, __ffma2_rn(dxa, dxa, nrc)));
       const float2 db = __ffma2_rn(dzb, dzb, __ffma2_rn(dyb, dyb, __ffma2_rn(dxb, dxb, nrc)));
+      // hit = sign bit of r^2 - rc^2 (1 + 2^-10); a -0 or NaN sign only admits a
+      // candidate that phase 2's exact test then drops
+      const uint32_t h0 = __float_as_uint(da.x) >> 31, h1 = __float_as_uint(da.y) >> 31;
+      const uint32_t h2 = __float_as_uint(db.x) >> 31, h3 = __float_as_uint(db.y) >> 31;
+      const uint32_t c1 = h0, c2 = h0 + h1, c3 = c2 + h2, c4 = c3 + h3;
       const uint32_t s = quad * 4u;
       sts_u16(oa, s);
-      oa += da.x < 0.0f ? 64u : 0u;
-      sts_u16(oa, s + 1u);
-      oa += da.y < 0.0f ? 64u : 0u;
-      sts_u16(oa, s + 2u);
-      oa += db.x < 0.0f ? 64u : 0u;
-      sts_u16(oa, s + 3u);
-      oa += db.y < 0.0f ? 64u : 0u;
+      sts_u16(oa + 64u * c1, s + 1u);
+      sts_u16(oa + 64u * c2, s + 2u);
+      sts_u16(oa + 64u * c3, s + 3u);
+      oa += 64u * c4;
+    };
+    if (nsteps == (uint32_t)(kChunk / 4)) {
+#pragma unroll
+      for (int kk = 0; kk < kChunk / 4; ++kk) test_quad(quads[kk]);
+    } else {
+#pragma unroll
+      for (int kk = 0; kk < kChunk / 4; ++kk) {
+        if ((uint32_t)kk >= nsteps) break;
+        test_quad(quads[kk]);
+      }
     }
   }
   flush((oa - lbase) >> 6);

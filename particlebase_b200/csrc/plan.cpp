@@ -72,7 +72,7 @@ static const char *env_once(int slot) {
   return v[slot];
 }
 
-int choose_segment(double atoms_per_cell, int nz, double scale, int nt) {
+int choose_segment(double atoms_per_cell, int nz, double scale, int nt, bool half) {
   // about 200 home atoms (25 clusters of 8) per force work item; PB_FORCE_SEG
   // overrides.  Shorter runs while the stage would not let two force CTAs
   // share an SM.
@@ -81,8 +81,11 @@ int choose_segment(double atoms_per_cell, int nz, double scale, int nt) {
   if (const char *e = env_once(0)) seg = std::atoi(e);
   seg = std::max(1, std::min(seg, force_max_segment()));
   seg = std::min(seg, nz);
+  // the kernel that runs sets the limit; the full-shell one also serves the
+  // soft-core and relaxation forces, so it always has to fit
   while (seg > 1 && (force_smem_per_cta(choose_capacity(apc, seg), nt) > 112 * 1024 ||
-                     force_half_smem_per_cta(choose_capacity_half(apc, seg), nt) > 112 * 1024))
+                     (half && force_half_smem_per_cta(choose_capacity_half(apc, seg), nt) >
+                                  112 * 1024)))
     --seg;
   return seg;
 }

@@ -27,7 +27,9 @@ void neighbor_table(const Grid &g, std::vector<uint32_t> &out);
 // z cells per force work item for a mean cell occupancy: about 200 * scale
 // home atoms per item, at most force_max_segment(), and short enough for two
 // force CTAs per SM with `nt` atom types.
-int choose_segment(double atoms_per_cell, int nz, double scale = 1.0, int nt = 1);
+// `half`: the half-shell force kernel runs (its stage has to fit as well).
+int choose_segment(double atoms_per_cell, int nz, double scale = 1.0, int nt = 1,
+                   bool half = false);
 
 // Shared-memory capacity (atoms) of a force CTA staging 9 columns x (seg + 2)
 // cells at the given mean occupancy, with headroom for fluctuations.
