@@ -142,15 +142,25 @@ __global__ void __launch_bounds__(256) k_scatter(CellBufs b) {
   b.pid_tmp[b.start[b.key[i]] + b.within[i]] = i;
 }
 
-// SoA mirror of sorted slot s (atom `me`): the system's sorted atom s - atom0
-// goes to mirror0 + (s - atom0).
+// SoA mirror of sorted slot s (atom `me`, cell `key`): the system's sorted
+// atom s - atom0 goes to mirror0 + (s - atom0).  An atom with a NaN or
+// infinite coordinate (a simulation that has blown up) is mirrored far away
+// in x and y, at the top edge of its cell in z, so that the force kernel never
+// finds it within range while every column stays sorted in z.
 __device__ __forceinline__ void write_mirror(const CellBufs &b, uint32_t me, uint32_t s,
-                                             const float4 &p) {
+                                             const float4 &p, uint32_t key) {
   const SysDesc &S = b.sys[system_of(b, me)];
   const uint32_t m = S.mirror0 + (s - S.atom0);
-  b.xs[m] = p.x;
-  b.ys[m] = p.y;
-  b.zs[m] = p.z;
+  float x = p.x, y = p.y, z = p.z;
+  if (!isfinite(x) || !isfinite(y) || !isfinite(z)) {
+    const uint32_t d2 = (key - S.cell0) % (uint32_t)S.g.n[2];
+    x = 1e30f;
+    y = 1e30f;
+    z = S.g.lo[2] + (float)(d2 + 1) * S.g.len[2];
+  }
+  b.xs[m] = x;
+  b.ys[m] = y;
+  b.zs[m] = z;
   b.ts[m] = (uint32_t)b.type[me];
 }
 
@@ -175,7 +185,7 @@ __device__ __forceinline__ bool canon_before(uint32_t ka, uint32_t a, uint32_t k
 // of a member is the number of members before it in that order, which orders
 // each cell canonically without depending on the atomic tickets of k_bin.
 __device__ __forceinline__ void canon_cell(const CellBufs &b, uint32_t s0, uint32_t n, int li,
-                                           int base, uint32_t lanes_n) {
+                                           int base, uint32_t lanes_n, uint32_t key) {
   const uint32_t me = li < (int)n ? b.pid_tmp[s0 + li] : kNone;
   const float4 p = li < (int)n ? b.r[me] : make_float4(0.f, 0.f, 0.f, 0.f);
   const uint32_t kz = z_key(p.z);
@@ -190,12 +200,12 @@ __device__ __forceinline__ void canon_cell(const CellBufs &b, uint32_t s0, uint3
     b.pid[s] = me;
     b.slot[me] = s;
     b.rs[s] = make_float4(p.x, p.y, p.z, __int_as_float((int)b.type[me]));
-    if (b.xs) write_mirror(b, me, s, p);
+    if (b.xs) write_mirror(b, me, s, p, key);
   }
 }
 
 // Cells with more than 32 members: O(n^2 / 32) ranking straight from global memory.
-__device__ void canon_large(const CellBufs &b, uint32_t s0, uint32_t n, int lane) {
+__device__ void canon_large(const CellBufs &b, uint32_t s0, uint32_t n, int lane, uint32_t key) {
   for (uint32_t a = lane; a < n; a += 32) {
     const uint32_t me = b.pid_tmp[s0 + a];
     const float4 p = b.r[me];
@@ -209,7 +219,7 @@ __device__ void canon_large(const CellBufs &b, uint32_t s0, uint32_t n, int lane
     b.pid[s] = me;
     b.slot[me] = s;
     b.rs[s] = make_float4(p.x, p.y, p.z, __int_as_float((int)b.type[me]));
-    if (b.xs) write_mirror(b, me, s, p);
+    if (b.xs) write_mirror(b, me, s, p, key);
   }
 }
 
@@ -228,15 +238,16 @@ __global__ void __launch_bounds__(256) k_canon(CellBufs b) {
   const uint32_t n0 = s1 - s0, n1 = s2 - s1;
   if (n0 <= 16 && n1 <= 16) {
     const int half = lane >> 4;
-    canon_cell(b, half ? s1 : s0, half ? n1 : n0, lane & 15, half * 16, max(n0, n1));
+    canon_cell(b, half ? s1 : s0, half ? n1 : n0, lane & 15, half * 16, max(n0, n1),
+               c0 + (uint32_t)half);
     return;
   }
   for (int k = 0; k < (two ? 2 : 1); ++k) {
     const uint32_t sb = k ? s1 : s0, n = k ? n1 : n0;
     if (n <= 32)
-      canon_cell(b, sb, n, lane, 0, n);
+      canon_cell(b, sb, n, lane, 0, n, c0 + (uint32_t)k);
     else
-      canon_large(b, sb, n, lane);
+      canon_large(b, sb, n, lane, c0 + (uint32_t)k);
   }
 }
 
