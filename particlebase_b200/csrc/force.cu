@@ -711,6 +711,160 @@ __device__ __forceinline__ void consume_cluster(const ForceBufs &b, const ItemDe
   }
 }
 
+// One cluster, one atom type, FP32 sums, LJ or capped law.  Phase 1 tests
+// the quads as consume_cluster does but appends a quad, not a candidate: one
+// 4-byte entry per quad with at least one admitted candidate, in a per-lane
+// list laid out lane-minor (entry k of lane l at 128 k + 4 l, one bank per
+// lane).  Phase 2 evaluates the 4 candidates of every listed quad in packed
+// FP32x2 and keeps the ones inside the exact cutoff; a far atom of the quad
+// (a run's padding) has r^2 = +inf and is dropped by the same test.
+template <bool ENERGY, int MODE>
+__device__ __forceinline__ void consume_cluster_quads(const ForceBufs &b, const ItemDesc<1> &d,
+                                                      const Planes &pl, uint32_t cl,
+                                                      uint16_t *mylist, uint16_t *tb,
+                                                      double (&ce)[4]) {
+  constexpr uint32_t kEntries = kListLen / 2;  // 4-byte entries per lane
+  const int lane = threadIdx.x & 31;
+  const int il = lane & 7, q = lane >> 3;
+  const float *X = pl.X, *Y = pl.Y, *Z = pl.Z;
+  const uint32_t H = d.H, hb = d.hb;
+  const uint32_t h = cl * 8 + il;
+  const bool valid = h < H;
+  const uint32_t hs = hb + (valid ? h : H - 1);
+  const float xi = valid ? X[hs] : kNoAtom;
+  const float yi = valid ? Y[hs] : kNoAtom;
+  const float zi = valid ? Z[hs] : kNoAtom;
+  const uint32_t pi = valid && q == 0 ? __ldg(b.pid + d.home_g0 + h) : 0u;
+  const uint32_t Q = d.Q[cl], M = d.M[cl];
+  const uint32_t magic = 0xffffffffu / M + 1u;
+  for (uint32_t idx = lane; idx < 9u * M; idx += 32) {
+    const uint32_t c = __umulhi(idx, magic), i = idx - c * M;
+    if (i < d.len[cl][c]) tb[table_pos(d.pre[cl][c] + i)] = (uint16_t)(d.q0[cl][c] + i);
+  }
+  for (uint32_t u = Q + lane; u < ((Q + 15u) & ~15u); u += 32)
+    tb[table_pos(u)] = (uint16_t)d.sentinel;
+  __syncwarp();
+
+  const float rc2 = d.lj.rc2[0];
+  const float2 nrc = make_float2(-rc2 * (1.0f + 1.0f / 1024.0f), -rc2 * (1.0f + 1.0f / 1024.0f));
+  const float2 m1 = make_float2(-1.0f, -1.0f), two = make_float2(2.0f, 2.0f);
+  const float2 half = make_float2(0.5f, 0.5f);
+  const float2 s2 = make_float2(d.lj.s2[0], d.lj.s2[0]);
+  const float2 e24 = make_float2(d.lj.e24[0], d.lj.e24[0]);
+  const float2 e4 = make_float2(d.lj.e4[0], d.lj.e4[0]);
+  const float ush = d.lj.ush[0];
+  const float2 xi2 = make_float2(xi, xi), yi2 = make_float2(yi, yi), zi2 = make_float2(zi, zi);
+  const uint32_t xa = smem_u32(X), ya = smem_u32(Y), za = smem_u32(Z);
+  const uint32_t lbase = smem_u32(mylist) + 4u * (uint32_t)lane;
+  PairAcc2<ENERGY> a;
+  // two candidates of a listed quad: force (and energy) inside the exact cutoff
+  auto pair2 = [&](float2 dx, float2 dy, float2 dz) {
+    const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+    const bool ina = r2.x < rc2 && r2.x > 0.0f, inb = r2.y < rc2 && r2.y > 0.0f;
+    float2 r2c = r2;
+    if (MODE == kModeCapped) {
+      const float2 fl = __fmul2_rn(make_float2(0.25f, 0.25f), s2);
+      r2c = make_float2(fmaxf(r2.x, fl.x), fmaxf(r2.y, fl.y));
+    }
+    const float2 inv = make_float2(rcp_approx(r2c.x), rcp_approx(r2c.y));
+    const float2 sr2 = __fmul2_rn(s2, inv);
+    const float2 sr6 = __fmul2_rn(__fmul2_rn(sr2, sr2), sr2);
+    const float2 t = __ffma2_rn(two, sr6, m1);
+    float2 f = __fmul2_rn(__fmul2_rn(__fmul2_rn(e24, sr6), t), inv);
+    f.x = ina ? f.x : 0.0f;
+    f.y = inb ? f.y : 0.0f;
+    a.fx = __ffma2_rn(f, dx, a.fx);
+    a.fy = __ffma2_rn(f, dy, a.fy);
+    a.fz = __ffma2_rn(f, dz, a.fz);
+    if (ENERGY) {
+      float2 u = __fmul2_rn(__fmul2_rn(e4, sr6), __fadd2_rn(sr6, m1));
+      u.x = ina ? u.x : 0.0f;
+      u.y = inb ? u.y : 0.0f;
+      float2 us = __fadd2_rn(u, make_float2(-ush, -ush));
+      us.x = ina ? us.x : 0.0f;
+      us.y = inb ? us.y : 0.0f;
+      a.pe = __ffma2_rn(half, u, a.pe);
+      a.pes = __ffma2_rn(half, us, a.pes);
+      // f is zero outside the cutoff, where r^2 may be +inf
+      float2 w = __fmul2_rn(__fmul2_rn(half, f), r2c);
+      w.x = ina ? w.x : 0.0f;
+      w.y = inb ? w.y : 0.0f;
+      a.vir = __fadd2_rn(a.vir, w);
+      a.n += (uint32_t)ina + (uint32_t)inb;
+    }
+  };
+  auto flush = [&](uint32_t cnt) {
+    const uint32_t steps = __reduce_max_sync(0xffffffffu, cnt);
+    for (uint32_t k = 0; k < steps; ++k) {
+      const uint32_t quad = k < cnt ? lds_u32(lbase + 128u * k) : d.sentinel;
+      const float4 x4 = lds_f4(xa + quad * 16u), y4 = lds_f4(ya + quad * 16u),
+                   z4 = lds_f4(za + quad * 16u);
+      pair2(__ffma2_rn(make_float2(x4.x, x4.y), m1, xi2),
+            __ffma2_rn(make_float2(y4.x, y4.y), m1, yi2),
+            __ffma2_rn(make_float2(z4.x, z4.y), m1, zi2));
+      pair2(__ffma2_rn(make_float2(x4.z, x4.w), m1, xi2),
+            __ffma2_rn(make_float2(y4.z, y4.w), m1, yi2),
+            __ffma2_rn(make_float2(z4.z, z4.w), m1, zi2));
+    }
+  };
+  uint32_t oa = lbase;  // shared-memory address of this lane's next entry
+  for (uint32_t u0 = 0; u0 < Q; u0 += kChunk) {
+    const uint32_t cnt = (oa - lbase) >> 7;
+    if (__reduce_max_sync(0xffffffffu, cnt) > kEntries - kChunk / 4) {
+      flush(cnt);
+      __syncwarp();
+      oa = lbase;
+    }
+    const uint2 qq = *reinterpret_cast<const uint2 *>(tb + u0 + 4 * q);
+    const uint32_t quads[4] = {qq.x & 0xffffu, qq.x >> 16, qq.y & 0xffffu, qq.y >> 16};
+    const uint32_t nsteps = min((Q - u0 + 3u) >> 2, (uint32_t)(kChunk / 4));
+    // one quad: 4 candidate tests; the quad is stored, and kept when any
+    // candidate is admitted (sign bit of r^2 - rc^2 (1 + 2^-10))
+    auto test_quad = [&](uint32_t quad) {
+      const float4 x4 = lds_f4(xa + quad * 16u), y4 = lds_f4(ya + quad * 16u),
+                   z4 = lds_f4(za + quad * 16u);
+      const float2 dxa = __ffma2_rn(make_float2(x4.x, x4.y), m1, xi2);
+      const float2 dxb = __ffma2_rn(make_float2(x4.z, x4.w), m1, xi2);
+      const float2 dya = __ffma2_rn(make_float2(y4.x, y4.y), m1, yi2);
+      const float2 dyb = __ffma2_rn(make_float2(y4.z, y4.w), m1, yi2);
+      const float2 dza = __ffma2_rn(make_float2(z4.x, z4.y), m1, zi2);
+      const float2 dzb = __ffma2_rn(make_float2(z4.z, z4.w), m1, zi2);
+      const float2 da = __ffma2_rn(dza, dza, __ffma2_rn(dya, dya, __ffma2_rn(dxa, dxa, nrc)));
+      const float2 db = __ffma2_rn(dzb, dzb, __ffma2_rn(dyb, dyb, __ffma2_rn(dxb, dxb, nrc)));
+      const uint32_t any = (__float_as_uint(da.x) | __float_as_uint(da.y) |
+                            __float_as_uint(db.x) | __float_as_uint(db.y)) >> 31;
+      sts_u32(oa, quad);
+      oa += any << 7;
+    };
+    if (nsteps == (uint32_t)(kChunk / 4)) {
+#pragma unroll
+      for (int kk = 0; kk < kChunk / 4; ++kk) test_quad(quads[kk]);
+    } else {
+#pragma unroll
+      for (int kk = 0; kk < kChunk / 4; ++kk) {
+        if ((uint32_t)kk >= nsteps) break;
+        test_quad(quads[kk]);
+      }
+    }
+  }
+  flush((oa - lbase) >> 7);
+  __syncwarp();
+  float fx = a.fx.x + a.fx.y, fy = a.fy.x + a.fy.y, fz = a.fz.x + a.fz.y;
+#pragma unroll
+  for (int o = 8; o < 32; o <<= 1) {
+    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+  }
+  if (valid && q == 0) b.F[pi] = make_float4(fx, fy, fz, 0.0f);
+  if (ENERGY) {
+    ce[0] = warp_sum((double)(a.pe.x + a.pe.y));
+    ce[1] = warp_sum((double)(a.pes.x + a.pes.y));
+    ce[2] = warp_sum((double)(a.vir.x + a.vir.y));
+    ce[3] = (double)warp_sum(a.n);
+  }
+}
+
 // Global-memory path of an item whose stage does not fit: task t covers the
 // groups of 32 consecutive home atoms t, t + ntask, ...; lanes are atoms.
 template <int NT, bool ENERGY, typename Acc, int MODE>
@@ -903,7 +1057,10 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
         const uint32_t first = ((uint32_t)cw + (uint32_t)kCons - d.base) % (uint32_t)kCons;
         for (uint32_t cl = first; cl < d.nclus; cl += kCons) {
           double ce[4];
-          consume_cluster<NT, ENERGY, Acc, MODE>(b, d, pbuf, cl, mylist, tb, ce);
+          if constexpr (NT == 1 && std::is_same<Acc, float>::value && MODE != kModeSoftCore)
+            consume_cluster_quads<ENERGY, MODE>(b, d, pbuf, cl, mylist, tb, ce);
+          else
+            consume_cluster<NT, ENERGY, Acc, MODE>(b, d, pbuf, cl, mylist, tb, ce);
           if (ENERGY && lane == 0)
             for (int k = 0; k < 4; ++k) cle[bf][cl][k] = ce[k];
         }
@@ -998,6 +1155,11 @@ int force_max_capacity(int warps, int nt) {
 
 int force_smem_per_cta(int cap, int nt) {
   return (int)smem_bytes((uint32_t)cap, kConsDefault, nt) + 15 * 1024;
+}
+
+int force_smem_limit() {
+  // two CTAs per SM share its 228 KB, less 1 KB per CTA reserved by the driver
+  return 112 * 1024;
 }
 
 int force_threads() { return 256; }

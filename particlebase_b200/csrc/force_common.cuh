@@ -69,6 +69,16 @@ __device__ __forceinline__ void sts_u16(uint32_t a, uint32_t v) {
   asm volatile("st.shared.u16 [%0], %1;" ::"r"(a), "h"((unsigned short)v) : "memory");
 }
 
+__device__ __forceinline__ uint32_t lds_u32(uint32_t a) {
+  uint32_t v;
+  asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void sts_u32(uint32_t a, uint32_t v) {
+  asm volatile("st.shared.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+
 // Position of flat quad u in a warp's quad table: within each chunk of 16,
 // the 4 quads lane q tests (u = q, q + 4, q + 8, q + 12) are adjacent, so a
 // lane fetches a chunk's quads with one 8-byte load.

@@ -83,7 +83,7 @@ int choose_segment(double atoms_per_cell, int nz, double scale, int nt, bool hal
   seg = std::min(seg, nz);
   // the kernel that runs sets the limit; the full-shell one also serves the
   // soft-core and relaxation forces, so it always has to fit
-  while (seg > 1 && (force_smem_per_cta(choose_capacity(apc, seg), nt) > 112 * 1024 ||
+  while (seg > 1 && (force_smem_per_cta(choose_capacity(apc, seg), nt) > force_smem_limit() ||
                      (half && force_half_smem_per_cta(choose_capacity_half(apc, seg), nt) >
                                   112 * 1024)))
     --seg;

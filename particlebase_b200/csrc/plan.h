@@ -49,6 +49,9 @@ int force_max_capacity(int warps, int nt);
 // Shared memory (dynamic plus an upper bound of the static part) of one
 // default-shape force CTA with staged-atom capacity `cap` and `nt` types.
 int force_smem_per_cta(int cap, int nt);
+// The shared memory a default-shape force CTA may use so that the CTAs per SM
+// its launch shape is built for stay resident.
+int force_smem_limit();
 // The same two for the half-shell force kernel (force_half.cu).
 int force_half_max_capacity(int nt);
 int force_half_smem_per_cta(int cap, int nt);
