@@ -54,10 +54,12 @@ def sources() -> list[str]:
 
 
 def _digest(paths: list[str], extra: str) -> str:
-    h = hashlib.sha256(extra.encode())
+    """Content digest of the sources and flags, with paths taken relative to
+    the repository, so that a copy of the tree elsewhere keeps its build."""
+    h = hashlib.sha256(extra.replace(ROOT, "<root>").encode())
     for p in paths:
         with open(p, "rb") as fh:
-            h.update(p.encode())
+            h.update(os.path.relpath(p, ROOT).encode())
             h.update(fh.read())
     return h.hexdigest()
 

@@ -399,15 +399,25 @@ int pb_batch_set_tuning(pb_batch *b, int force_threads, float seg_scale) {
 int pb_batch_estimate_bytes(const uint32_t *natoms, const float *cells6, const float *rmax,
                             uint32_t nsys, uint32_t flags, size_t *bytes) {
   if (!natoms || !cells6 || !rmax || !bytes || nsys == 0) return PB_ERR_ARG;
-  // per atom: r, F[2], rs (16 B each), minv, mass, key, within, pid_tmp, pid,
-  // slot (4 B each), x, y, z, type mirrors of rs (16 B), type (2 B),
-  // velocities (16 or 24 B), sysid (4 B), fixed-point force sums (48 B)
-  const size_t per_atom = 16 * 4 + 4 * 7 + 16 + 2 + ((flags & PB_MD_VEL_FP64) ? 24 : 16) +
+  // per atom: r, F[2], rs (16 B each), minv, mass, key, pid_tmp, pid, slot
+  // (4 B each), the overflow list entry (8 B), x, y, z, type mirrors of rs
+  // (16 B), type (2 B), velocities (16 or 24 B), sysid (4 B), fixed-point
+  // force sums (48 B)
+  const size_t per_atom = 16 * 4 + 4 * 6 + 8 + 16 + 2 + ((flags & PB_MD_VEL_FP64) ? 24 : 16) +
                           (nsys > 1 ? 4 : 0) + 48;
+  // per cell: the bucket, sized by the densest system as the engine does
+  double apc_max = 0.0;
+  for (uint32_t s = 0; s < nsys; ++s) {
+    Grid g;
+    if (!make_grid(cells6 + 6 * s, rmax[s], g)) return PB_ERR_ARG;
+    apc_max = std::max(apc_max, (double)natoms[s] / g.ncells);
+  }
+  const size_t per_cell_bucket = 4 * (size_t)choose_bucket_cap(apc_max) + 1;  // + tile count
   size_t total = 0;
   for (uint32_t s = 0; s < nsys; ++s) {
     Grid g;
     if (!make_grid(cells6 + 6 * s, rmax[s], g)) return PB_ERR_ARG;
+    total += per_cell_bucket * (size_t)g.ncells;
     const size_t cols = (size_t)g.n[0] * g.n[1];
     const size_t items = cols * (size_t)(2 + g.n[2] / 4);  // generous: runs per column
     const size_t blocks = blocks_for(natoms[s]);

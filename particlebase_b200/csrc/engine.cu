@@ -121,10 +121,12 @@ std::shared_ptr<const Plan> cached_plan(const Grid &g, int seg) {
 
 void free_cells(Engine &e) {
   dfree(e, e.key);
-  dfree(e, e.within);
   dfree(e, e.count);
   dfree(e, e.start);
-  dfree(e, e.tilesum);
+  dfree(e, e.bucket);
+  dfree(e, e.ovf);
+  dfree(e, e.tcount);
+  dfree(e, e.cctl);
   dfree(e, e.pid_tmp);
   dfree(e, e.pid);
   dfree(e, e.slot);
@@ -474,6 +476,7 @@ int engine_setup_cells(Engine &e) {
   uint32_t mirror = 0;
   e.cap_max = 0;
   e.cap_half_max = 0;
+  double apc_max = 0.0;
   // grids and plans first, so that the item and column arrays are sized once
   std::vector<std::shared_ptr<const Plan>> plans(e.nsys);
   size_t nitem_all = 0, ncol_all = 0;
@@ -485,6 +488,7 @@ int engine_setup_cells(Engine &e) {
       return fail(e, PB_ERR_ARG, "cell grid needs at least 3 cells per axis (blocknum > 2)");
     P.grid = g;
     const double apc = (double)P.n / g.ncells;
+    apc_max = std::max(apc_max, apc);
     const bool half = (e.flags & PB_MD_HALF_SHELL) && !(e.flags & PB_MD_ACC_FP64);
     P.seg = choose_segment(apc, g.n[2], e.seg_scale, P.lj_set ? P.lj.nt : 1, half);
     P.cap = (uint32_t)choose_capacity(apc, P.seg);
@@ -548,10 +552,15 @@ int engine_setup_cells(Engine &e) {
   e.nitems = (uint32_t)items.size();
   e.mirrorN = mirror + 4u;
   const uint32_t N = e.N, C = e.ncells;
-  const uint32_t ntiles = (C + 4095) / 4096;
-  bool ok = dalloc(e, &e.key, N) == cudaSuccess && dalloc(e, &e.within, N) == cudaSuccess &&
-            dalloc(e, &e.count, C) == cudaSuccess && dalloc(e, &e.start, (size_t)C + 1) == cudaSuccess &&
-            dalloc(e, &e.tilesum, ntiles) == cudaSuccess && dalloc(e, &e.pid_tmp, N) == cudaSuccess &&
+  e.bucket_cap = (uint32_t)choose_bucket_cap(apc_max);
+  e.ntile = (C + 63) / 64;
+  e.tile_atoms = (uint32_t)choose_tile_atoms(apc_max);
+  bool ok = dalloc(e, &e.key, N) == cudaSuccess && dalloc(e, &e.count, C) == cudaSuccess &&
+            dalloc(e, &e.start, (size_t)C + 1) == cudaSuccess &&
+            dalloc(e, &e.bucket, (size_t)C * e.bucket_cap) == cudaSuccess &&
+            dalloc(e, &e.ovf, N) == cudaSuccess &&
+            dalloc(e, &e.tcount, e.ntile) == cudaSuccess &&
+            dalloc(e, &e.cctl, 2) == cudaSuccess && dalloc(e, &e.pid_tmp, N) == cudaSuccess &&
             dalloc(e, &e.pid, N) == cudaSuccess && dalloc(e, &e.slot, N) == cudaSuccess &&
             dalloc(e, &e.rs, N) == cudaSuccess && dalloc(e, &e.xs, e.mirrorN) == cudaSuccess &&
             dalloc(e, &e.ys, e.mirrorN) == cudaSuccess && dalloc(e, &e.zs, e.mirrorN) == cudaSuccess &&
@@ -566,6 +575,8 @@ int engine_setup_cells(Engine &e) {
     return fail(e, PB_ERR_OOM, "cell list allocation failed");
   }
   E_CUDA(cudaMemsetAsync(e.count, 0, sizeof(uint32_t) * C, e.stream));
+  E_CUDA(cudaMemsetAsync(e.tcount, 0, sizeof(uint32_t) * e.ntile, e.stream));
+  E_CUDA(cudaMemsetAsync(e.cctl, 0, sizeof(uint32_t) * 2, e.stream));
   E_CUDA(cudaMemsetAsync(e.fqueue, 0, sizeof(uint32_t) * 2, e.stream));
   E_CUDA(cudaMemcpyAsync(e.colrank, rank_all.data(), 4 * rank_all.size(), cudaMemcpyHostToDevice,
                          e.stream));
@@ -623,11 +634,16 @@ CellBufs engine_cbufs(Engine &e) {
   b.N = e.N;
   b.ncells = e.ncells;
   b.key = e.key;
-  b.within = e.within;
   b.count = e.count;
   b.start = e.start;
-  b.tilesum = e.tilesum;
   b.pid_tmp = e.pid_tmp;
+  b.bucket = e.bucket;
+  b.bucket_cap = e.bucket_cap;
+  b.ovf = e.ovf;
+  b.tcount = e.tcount;
+  b.ntile = e.ntile;
+  b.tile_atoms = e.tile_atoms;
+  b.ctl = e.cctl;
   b.pid = e.pid;
   b.slot = e.slot;
   b.rs = e.rs;

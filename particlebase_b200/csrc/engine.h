@@ -62,9 +62,14 @@ struct Engine {
   // cell list (after setup_cells)
   bool cells_ready = false;
   uint32_t ncells = 0;
-  uint32_t *key = nullptr, *within = nullptr, *count = nullptr, *start = nullptr,
-           *tilesum = nullptr, *pid_tmp = nullptr, *pid = nullptr, *slot = nullptr,
-           *colrank = nullptr, *colxy = nullptr, *d_item0 = nullptr;
+  uint32_t *key = nullptr, *count = nullptr, *start = nullptr, *pid_tmp = nullptr,
+           *pid = nullptr, *slot = nullptr, *colrank = nullptr, *colxy = nullptr,
+           *d_item0 = nullptr;
+  // cell buckets of the two-kernel build: bucket_cap ids per cell, the
+  // overflow list, tile counts, and two control words
+  uint32_t *bucket = nullptr, *tcount = nullptr, *cctl = nullptr;
+  uint2 *ovf = nullptr;
+  uint32_t bucket_cap = 0, ntile = 0, tile_atoms = 0;
   float4 *rs = nullptr;
   float *xs = nullptr, *ys = nullptr, *zs = nullptr;  // SoA mirrors of rs
   uint32_t *ts = nullptr;

@@ -64,6 +64,14 @@ struct CellBufs {
   uint32_t ncells;           // packed cells over all systems
   uint32_t *key, *within, *count, *start, *tilesum;
   uint32_t *pid_tmp, *pid, *slot;
+  // two-kernel build (bucket == nullptr: the six-kernel counting sort)
+  uint32_t *bucket;          // per cell, bucket_cap member ids in ticket order
+  uint32_t bucket_cap;       // at least 32
+  uint2 *ovf;                // (cell, atom) of the members past bucket_cap; N entries
+  uint32_t *tcount;          // atoms per 64-cell tile
+  uint32_t ntile;
+  uint32_t tile_atoms;       // members a k_canon_tiles block stages in shared memory
+  uint32_t *ctl;             // [0] overflow entries, [1] finished k_canon_tiles blocks
   float4 *rs;
   // structure-of-arrays mirrors of rs (nullptr: not written); system s's
   // sorted atom k sits at mirror0 + k, so 16-byte runs align the same way

@@ -90,6 +90,18 @@ int choose_segment(double atoms_per_cell, int nz, double scale, int nt, bool hal
   return seg;
 }
 
+int choose_bucket_cap(double atoms_per_cell) {
+  const double want = 2.0 * std::max(atoms_per_cell, 0.0) + 8.0;
+  const int cap = ((int)std::ceil(want) + 7) & ~7;
+  return std::max(32, std::min(cap, 1024));
+}
+
+int choose_tile_atoms(double atoms_per_cell) {
+  const double want = 64.0 * 1.3 * std::max(atoms_per_cell, 0.0) + 64.0;
+  const int n = ((int)std::ceil(want) + 31) & ~31;
+  return std::max(256, std::min(n, 4096));
+}
+
 int choose_capacity(double atoms_per_cell, int seg) {
   const double expect = 9.0 * (seg + 2) * std::max(atoms_per_cell, 1.0);
   double factor = 1.15;  // headroom over the mean occupancy; PB_FORCE_CAP overrides

@@ -34,6 +34,12 @@ int choose_segment(double atoms_per_cell, int nz, double scale = 1.0, int nt = 1
 // Shared-memory capacity (atoms) of a force CTA staging 9 columns x (seg + 2)
 // cells at the given mean occupancy, with headroom for fluctuations.
 int choose_capacity(double atoms_per_cell, int seg);
+// Member slots per cell bucket of the two-kernel cell build: at least 32 and
+// about twice the mean occupancy (a fuller cell spills to the overflow list).
+int choose_bucket_cap(double atoms_per_cell);
+// Members a 64-cell tile block of the cell build stages in shared memory
+// (9 B each): about 1.3 times the mean tile; fuller tiles take the slower path.
+int choose_tile_atoms(double atoms_per_cell);
 // The same for the half-shell force kernel, which stages 5 columns.
 int choose_capacity_half(double atoms_per_cell, int seg);
 
