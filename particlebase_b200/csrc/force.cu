@@ -94,8 +94,8 @@ struct Scratch {
   uint32_t gstart[9][kMaxSeg + 3];
   uint32_t cnt[9][kMaxSeg + 3];
   uint32_t dst[27], lead[27], n[27], alen[27];
+  uint32_t src[27];    // mirror slot of each run's first (16-byte aligned) slot
   float shift[27][3];  // frame shift of each run
-  uint32_t shifted;    // runs with a nonzero shift (bit 3 c + p)
 };
 
 // Slots of a stage buffer for `cap` staged atoms: each of up to 3 copy runs
@@ -284,8 +284,7 @@ __device__ __forceinline__ void flush_packed(const float *X, const float *Y, con
 // gave up.
 template <int NT, int MODE, int kProd, int kCons>
 __device__ bool produce_item(const ForceBufs &b, uint32_t item, ItemDesc<NT> &d, Scratch &sc,
-                             const Planes &pl, uint64_t *landed, uint32_t &lphase,
-                             uint32_t &running) {
+                             const Planes &pl, uint32_t &running) {
   constexpr int kPT = kProd * 32;  // producer threads
   const int pt = threadIdx.x, lane = pt & 31, pw = pt >> 5;
   const ForceItem it = b.items[item];
@@ -406,6 +405,7 @@ __device__ bool produce_item(const ForceBufs &b, uint32_t item, ItemDesc<NT> &d,
       ry = d.sy[c];
       rz = pp == 0 ? sz_lo : (pp == 1 ? Fz : sz_hi);
       sc.dst[lane] = dst;
+      sc.src[lane] = ma;
       sc.lead[lane] = m0 - ma;
       sc.n[lane] = n;
       sc.alen[lane] = alen;
@@ -414,9 +414,6 @@ __device__ bool produce_item(const ForceBufs &b, uint32_t item, ItemDesc<NT> &d,
       sc.shift[lane][2] = rz;
       if (lane % 3 == 0) d.ps[lane / 3] = dst;
     }
-    const uint32_t shifted =
-        __ballot_sync(0xffffffffu, n > 0 && (rx != 0.f || ry != 0.f || rz != 0.f));
-    if (lane == 0) sc.shifted = shifted;
     // the system's own capacity decides: the same path alone or batched
     const bool overflow = total + 4u > padded_slots(scap) || nclus > (uint32_t)kWinCap;
     if (lane == 0) {
@@ -429,44 +426,44 @@ __device__ bool produce_item(const ForceBufs &b, uint32_t item, ItemDesc<NT> &d,
         atomicOr(&b.status[it.sys], kStatusSmemOverflow);
       }
     }
-    if (!overflow && total > 0) {
-      uint32_t bytes = alen * 4u * (NT > 1 ? 4u : 3u);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
-      if (lane == 0) mbar_arrive_expect_tx(landed, bytes);
-      __syncwarp();
-      if (lane < 27 && alen > 0) {
-        bulk_g2s(pl.X + dst, b.xs + ma, alen * 4u, landed);
-        bulk_g2s(pl.Y + dst, b.ys + ma, alen * 4u, landed);
-        bulk_g2s(pl.Z + dst, b.zs + ma, alen * 4u, landed);
-        if (NT > 1) bulk_g2s(pl.T + dst, b.ts + ma, alen * 4u, landed);
-      }
-    }
   }
   producer_sync<kProd>();
   if (d.overflow) return true;
   const uint32_t total = d.ps[9];
   if (total > 0) {
-    bool ok = pt != 0 || mbar_wait_or_abort(landed, lphase, &kNeverAbort);
-    lphase ^= 1u;
-    // all producer threads learn the outcome through the barrier
-    if (pt == 0 && !ok) {
-      atomicOr(&b.status[it.sys], kStatusWaitTimeout);
-      // give the copies in flight a second bounded wait before giving up
-      mbar_wait_bounded(landed, lphase ^ 1u);
-      d.skip = 2;
-    }
-    producer_sync<kProd>();
-    if (d.skip == 2) return false;
-    // frame shifts of the real atoms of the shifted runs
-    for (uint32_t m = sc.shifted; m != 0u; m &= m - 1u) {
-      const int p = __ffs(m) - 1;
-      const float sx = sc.shift[p][0], sy = sc.shift[p][1], sz = sc.shift[p][2];
-      const uint32_t s0 = sc.dst[p] + sc.lead[p], s1 = s0 + sc.n[p];
-      for (uint32_t s = s0 + pt; s < s1; s += kPT) {
-        pl.X[s] -= sx;
-        pl.Y[s] -= sy;
-        pl.Z[s] -= sz;
+    // the runs' 16-byte quads, all producer threads, each run moved into the
+    // item's frame on the way (x - 0 is x, so unshifted runs pass unchanged);
+    // kCopyBatch quads per thread are loaded before any is stored
+    constexpr int kB = NT > 1 ? kCopyBatch / 2 : kCopyBatch;  // the type plane takes registers
+    const uint32_t nq = total >> 2;
+    int p = 0;
+    for (uint32_t u0 = pt; u0 < nq; u0 += kB * kPT) {
+      float4 vx[kB], vy[kB], vz[kB];
+      uint4 vt[NT > 1 ? kB : 1];
+      int pr[kB];
+#pragma unroll
+      for (int k = 0; k < kB; ++k) {
+        const uint32_t u = u0 + (uint32_t)k * kPT;
+        pr[k] = -1;
+        if (u < nq) {
+          while (4u * u >= sc.dst[p] + sc.alen[p]) ++p;  // runs in slot order
+          pr[k] = p;
+          const uint32_t g = sc.src[p] + (4u * u - sc.dst[p]);
+          vx[k] = ldg_f4(b.xs + g);
+          vy[k] = ldg_f4(b.ys + g);
+          vz[k] = ldg_f4(b.zs + g);
+          if (NT > 1) vt[k] = ldg_u4(b.ts + g);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kB; ++k) {
+        if (pr[k] < 0) break;
+        const uint32_t s = 4u * (u0 + (uint32_t)k * kPT);
+        const float sx = sc.shift[pr[k]][0], sy = sc.shift[pr[k]][1], sz = sc.shift[pr[k]][2];
+        sts_f4(smem_u32(pl.X + s), make_float4(vx[k].x - sx, vx[k].y - sx, vx[k].z - sx, vx[k].w - sx));
+        sts_f4(smem_u32(pl.Y + s), make_float4(vy[k].x - sy, vy[k].y - sy, vy[k].z - sy, vy[k].w - sy));
+        sts_f4(smem_u32(pl.Z + s), make_float4(vz[k].x - sz, vz[k].y - sz, vz[k].z - sz, vz[k].w - sz));
+        if (NT > 1) *reinterpret_cast<uint4 *>(pl.T + s) = vt[k];
       }
     }
     producer_sync<kProd>();
@@ -926,7 +923,7 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ ItemDesc<NT> desc[2];
   __shared__ Scratch sc;
-  __shared__ uint64_t full[2], empty[2], landed[2];
+  __shared__ uint64_t full[2], empty[2];
   __shared__ double cle[2][kWinCap][4];
   __shared__ int abort_flag, wait_ok;
   __shared__ uint32_t next_item;
@@ -949,7 +946,6 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
     for (int k = 0; k < 2; ++k) {
       mbar_init(&full[k], 1);
       mbar_init(&empty[k], kCons);
-      mbar_init(&landed[k], 1);
     }
     abort_flag = 0;
     mbar_fence_init();
@@ -988,7 +984,7 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
         }
       }
     };
-    uint32_t lphase0 = 0u, lphase1 = 0u, running = 0;
+    uint32_t running = 0;
     uint32_t n = 0;
     for (;; ++n) {
       if (threadIdx.x == 0) next_item = atomicAdd(b.queue, 1u);
@@ -1014,7 +1010,7 @@ __global__ void __launch_bounds__((kProd + kCons) * 32, (kProd + kCons) >= 16 ? 
         break;
       }
       const bool ok = produce_item<NT, MODE, kProd, kCons>(
-          b, item, desc[bf], sc, planes(bf), &landed[bf], bf ? lphase1 : lphase0, running);
+          b, item, desc[bf], sc, planes(bf), running);
       if (!ok) {
         done_claiming();
         if (threadIdx.x == 0) abort_flag = 1;
@@ -1153,8 +1149,19 @@ int force_max_capacity(int warps, int nt) {
   return (int)cap;
 }
 
+// Static shared memory of a force CTA for up to `nt` types: the two item
+// descriptors, the producer scratch, the per-cluster energy sums, and 1 KB
+// for barriers and flags.
+template <int NT>
+constexpr uint32_t static_smem() {
+  return 2u * (uint32_t)sizeof(ItemDesc<NT>) + (uint32_t)sizeof(Scratch) +
+         2u * kWinCap * 4u * 8u + 1024u;
+}
+
 int force_smem_per_cta(int cap, int nt) {
-  return (int)smem_bytes((uint32_t)cap, kConsDefault, nt) + 15 * 1024;
+  const uint32_t st = nt <= 1 ? static_smem<1>() : nt <= 2 ? static_smem<2>()
+                      : nt <= 4 ? static_smem<4>() : static_smem<8>();
+  return (int)(smem_bytes((uint32_t)cap, kConsDefault, nt) + st);
 }
 
 int force_smem_limit() {

@@ -15,6 +15,7 @@ namespace {
 
 constexpr int kMaxSeg = 32;     // longest z run of one work item (cells)
 constexpr int kListLen = 40;    // per-lane pair list entries
+constexpr int kCopyBatch = 4;   // stage quads a producer thread loads before storing
 constexpr int kChunk = 16;      // candidates a lane tests between list checks
 constexpr int kWinCap = 48;     // clusters (or global-path tasks) per item
 constexpr float kFar = 1e30f;   // pad-slot coordinate: never within range
@@ -49,6 +50,31 @@ __device__ __forceinline__ float4 lds_f4(uint32_t a) {
       : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
       : "r"(a));
   return v;
+}
+
+// Read-only global loads of 16 bytes (the sorted-position mirrors, which no
+// kernel writes while the force kernel runs).
+__device__ __forceinline__ float4 ldg_f4(const float *p) {
+  float4 v;
+  asm("ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+      : "l"(p));
+  return v;
+}
+
+__device__ __forceinline__ uint4 ldg_u4(const uint32_t *p) {
+  uint4 v;
+  asm("ld.global.nc.v4.u32 {%0, %1, %2, %3}, [%4];"
+      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+      : "l"(p));
+  return v;
+}
+
+// Stage stores of the producers (ordered before their barrier, which is
+// volatile too).
+__device__ __forceinline__ void sts_f4(uint32_t a, float4 v) {
+  asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(a), "f"(v.x), "f"(v.y), "f"(v.z),
+               "f"(v.w));
 }
 
 __device__ __forceinline__ float lds_f32(uint32_t a) {
