@@ -35,7 +35,11 @@ int field_slice(pb_batch *b, uint32_t s, int field, char **ptr, size_t *bytes, b
   Engine &e = b->e;
   const size_t a0 = e.atom0[s], n = e.sp[s].n;
   switch (field) {
-    case PB_FIELD_R: *ptr = (char *)(e.r + a0); *bytes = 16 * n; break;
+    case PB_FIELD_R:
+      *ptr = (char *)(e.r + a0);
+      *bytes = 16 * n;
+      if (for_set) e.sp[s].r_set = true;
+      break;
     case PB_FIELD_V:
       if (!e.v) return fail(b, PB_ERR_STATE, "batch keeps FP64 velocities");
       *ptr = (char *)(e.v + a0); *bytes = 16 * n; break;
@@ -134,6 +138,7 @@ int pb_batch_repack(const pb_batch *old, const int32_t *src, const uint32_t *nat
     P.kB = Q.kB;
     P.lj = Q.lj;
     P.lj_set = Q.lj_set;
+    P.r_set = Q.r_set;  // positions are gathered from the old batch
     P.lj_percut = Q.lj_percut;
     P.m0 = Q.m0;
     P.dt = Q.dt;

@@ -25,6 +25,7 @@ struct SysParams {
   uint32_t cap_half = 0;  // stage capacity of the half-shell force kernel
   double m0 = 1.0;
   float dt = 0.005f;
+  bool r_set = false;     // positions imported or set (the cell build may be timed)
   std::vector<uint32_t> key_of_ref, ref_of_key;  // reference cell id <-> packed key - cell0
 };
 
@@ -62,7 +63,8 @@ struct Engine {
   // cell list (after setup_cells)
   bool cells_ready = false;
   uint32_t ncells = 0;
-  uint32_t *key = nullptr, *count = nullptr, *start = nullptr, *pid_tmp = nullptr,
+  uint32_t *key = nullptr, *within = nullptr, *tilesum = nullptr, *count = nullptr,
+           *start = nullptr, *pid_tmp = nullptr,
            *pid = nullptr, *slot = nullptr, *colrank = nullptr, *colxy = nullptr,
            *d_item0 = nullptr;
   // cell buckets of the two-kernel build: bucket_cap ids per cell, the
@@ -70,6 +72,9 @@ struct Engine {
   uint32_t *bucket = nullptr, *tcount = nullptr, *cctl = nullptr;
   uint2 *ovf = nullptr;
   uint32_t bucket_cap = 0, ntile = 0, tile_atoms = 0;
+  // which cell build the steps use: the bucket build (true) or the six-kernel
+  // counting sort; chosen by timing both at cell set-up (same result bits)
+  bool cells_bucket = true;
   float4 *rs = nullptr;
   float *xs = nullptr, *ys = nullptr, *zs = nullptr;  // SoA mirrors of rs
   uint32_t *ts = nullptr;

@@ -434,7 +434,10 @@ int pb_md_set(pb_md *h, int field, const void *host, size_t bytes) {
   e.mv2_fresh = false;  // velocities or masses may change
   void *dst = nullptr;
   switch (field) {
-    case PB_FIELD_R: dst = e.r; break;
+    case PB_FIELD_R:
+      dst = e.r;
+      for (auto &P : e.sp) P.r_set = true;
+      break;
     case PB_FIELD_V: dst = e.v; break;
     case PB_FIELD_VD: dst = e.vd; break;
     case PB_FIELD_F: dst = e.F[e.last]; break;

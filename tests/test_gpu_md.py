@@ -83,6 +83,31 @@ def test_cells_bit_exact_1m(cuda_lib, po):
     check_cells(p, s, po)
 
 
+@pytest.mark.parametrize("shuffle", [False, True])
+def test_bucket_and_sort_builds_agree(cuda_lib, po, shuffle, monkeypatch):
+    """The engine picks the faster of its two cell builds at set-up; both must
+    give the same bits.  A 256,000-atom lattice in lattice order (the bucket
+    build's case) and in random particle order (the counting sort's), each
+    built both ways; the sorted layout, cell starts, force-kernel mirrors and
+    forces are compared, and the first build is checked against the oracle."""
+    s = perturbed(W.fcc_system(40, 0.8442, 0.72, seed=9), 0.1, 8)
+    if shuffle:
+        perm = np.random.default_rng(3).permutation(s.n)
+        s.r, s.v = s.r[perm], s.v[perm]
+    got = []
+    for mode in ("bucket", "sort"):
+        monkeypatch.setenv("PB_CELL_BUILD", mode)
+        p = md(cuda_lib, s)
+        p.calcBlockID()
+        p.calcForce()
+        if mode == "bucket":
+            check_cells(p, s, po)
+        got.append({f: p.get(f) for f in ("pid", "cell_start", "r_sorted", "F")})
+        p.close()
+    for f in got[0]:
+        assert np.array_equal(got[0][f], got[1][f]), f
+
+
 def test_force_c1_vs_oracle_and_reference(cuda_lib, po, golden):
     s = W.config_c1()
     s.r = golden["c1_r4"][:, :3].astype(np.float64)
