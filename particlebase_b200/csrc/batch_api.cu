@@ -108,6 +108,10 @@ int pb_batch_repack(const pb_batch *old, const int32_t *src, const uint32_t *nat
   }
   e.force_threads = o.force_threads;
   e.seg_scale = o.seg_scale;
+  // a repack keeps the cell build its source batch measured (the particle
+  // order of continuing systems does not change)
+  e.cells_bucket = o.cells_bucket;
+  e.cells_chosen = o.cells_chosen;
   auto bail = [&](int code) {
     engine_free(e);
     delete b;

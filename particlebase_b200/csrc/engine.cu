@@ -474,6 +474,7 @@ int engine_import(Engine &e, uint32_t sys, const double *r3, const double *v3, c
 // With positions in place and enough atoms to matter, both run twice on the
 // engine's stream and the faster is kept.
 void choose_cell_build(Engine &e) {
+  if (e.cells_chosen) return;
   e.cells_bucket = true;
   // PB_CELL_BUILD=bucket or sort fixes the choice (tests, measurements)
   if (const char *m = std::getenv("PB_CELL_BUILD")) {
@@ -503,6 +504,7 @@ void choose_cell_build(Engine &e) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   e.cells_bucket = !ok || t[0] <= t[1];
+  e.cells_chosen = ok;
 }
 
 int engine_setup_cells(Engine &e) {

@@ -75,6 +75,7 @@ struct Engine {
   // which cell build the steps use: the bucket build (true) or the six-kernel
   // counting sort; chosen by timing both at cell set-up (same result bits)
   bool cells_bucket = true;
+  bool cells_chosen = false;  // set: keep cells_bucket at the next set-up (repacks)
   float4 *rs = nullptr;
   float *xs = nullptr, *ys = nullptr, *zs = nullptr;  // SoA mirrors of rs
   uint32_t *ts = nullptr;
