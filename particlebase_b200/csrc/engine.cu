@@ -304,6 +304,8 @@ void engine_free(Engine &e) {
   dfree(e, e.sc);
   dfree(e, e.status);
   dfree(e, e.d_fac);
+  if (e.h_read) cudaFreeHost(e.h_read);
+  e.h_read = nullptr;
   dfree(e, e.facc);
   dfree(e, e.d_lj);
   dfree(e, e.steps_left);

@@ -58,6 +58,7 @@ struct Engine {
   DevScalars *sc = nullptr;
   uint32_t *status = nullptr;
   double *d_fac = nullptr;  // per-system factors for scale / adjust
+  double *h_read = nullptr;  // pinned host word for per-step scalar reads (lazy)
   LJTable *d_lj = nullptr;
 
   // cell list (after setup_cells)

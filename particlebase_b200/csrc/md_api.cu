@@ -314,11 +314,13 @@ int pb_md_temperature(pb_md *h, double *T) {
     const int rc = engine_mv2(h->e);
     if (rc) return rc;
   }
-  double mv2 = 0;
-  H_CUDA(cudaMemcpyAsync(&mv2, &h->e.sc[0].mv2, sizeof(double), cudaMemcpyDeviceToHost,
+  // a pinned word: the driver loop reads the temperature every step, and a
+  // copy to pageable memory goes through a staging buffer
+  if (!h->e.h_read) H_CUDA(cudaMallocHost(&h->e.h_read, sizeof(double)));
+  H_CUDA(cudaMemcpyAsync(h->e.h_read, &h->e.sc[0].mv2, sizeof(double), cudaMemcpyDeviceToHost,
                          h->e.stream));
   H_CUDA(cudaStreamSynchronize(h->e.stream));
-  *T = mv2 / (3.0 * h->e.N * h->p().kB);
+  *T = *h->e.h_read / (3.0 * h->e.N * h->p().kB);
   return PB_OK;
 }
 
