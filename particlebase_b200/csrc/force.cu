@@ -330,7 +330,10 @@ __device__ bool produce_item(const ForceBufs &b, uint32_t item, ItemDesc<NT> &d,
     d.sy[c] = Fy - (float)wy * g.L[1];
     d.kbase[c] = it.kbase[c];
   }
-  const float Fz = z1 == nz ? g.L[2] : 0.0f;
+  // an item on the top face works in the frame shifted down by L, where the
+  // shifts of its atoms (all in the upper half) are exact; a whole column
+  // keeps the unshifted frame and rounds only the image above its top
+  const float Fz = z1 == nz && z0 > 0 ? g.L[2] : 0.0f;
   const float sz_lo = z0 == 0 ? Fz + g.L[2] : Fz;  // image z0 - 1 wraps below when z0 == 0
   const float sz_hi = z1 == nz ? Fz - g.L[2] : Fz;  // image z1 wraps above when z1 == nz
   if (pt == 0) {

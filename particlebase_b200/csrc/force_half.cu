@@ -226,7 +226,10 @@ __device__ bool produce_item3(const ForceBufs &b, uint32_t item, ItemDesc3<NT> &
     d.sy[c] = Fy - (float)wy * g.L[1];
     d.kbase[c] = it.kbase[k9];
   }
-  const float Fz = z1 == nz ? g.L[2] : 0.0f;
+  // an item on the top face works in the frame shifted down by L, where the
+  // shifts of its atoms (all in the upper half) are exact; a whole column
+  // keeps the unshifted frame and rounds only the image above its top
+  const float Fz = z1 == nz && z0 > 0 ? g.L[2] : 0.0f;
   const float sz_lo = z0 == 0 ? Fz + g.L[2] : Fz;
   const float sz_hi = z1 == nz ? Fz - g.L[2] : Fz;
   if (pt == 0) {

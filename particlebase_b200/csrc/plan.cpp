@@ -130,9 +130,12 @@ void append_items(uint32_t sys, const Grid &g, int seg, uint32_t cell0,
                   std::vector<ForceItem> &items) {
   const uint32_t ncol = (uint32_t)g.n[0] * g.n[1];
   const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
-  const int t = std::max(1, std::min(seg, nz / 2 - 1));
+  // a column that fits one run is one item; otherwise a top run of at most
+  // nz / 2 - 1 cells (its frame shift is exact) and runs of at most seg below
+  const bool whole = nz <= seg;
+  const int t = whole ? nz : std::max(1, std::min(seg, nz / 2 - 1));
   const int rest = nz - t;
-  const int parts = std::max(1, (rest + seg - 1) / seg);
+  const int parts = whole ? 0 : std::max(1, (rest + seg - 1) / seg);
   for (uint32_t c = 0; c < ncol; ++c) {
     ForceItem it{};
     it.sys = sys;
