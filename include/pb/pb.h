@@ -135,7 +135,12 @@ int pb_md_import_arrays(pb_md *h, const double *r3, const double *v3, const doub
                         const uint32_t *type);
 /* cudaParticleMD::setupCutoffBlock -> cudaCutoffBlock::setupCutoffBlock +
  * setupSortedPositions (cudaParticleMD.hh:71-74, cudaCutoffBlock.cu:75-231).
- * Only periodic boxes are supported (periodic = 0 -> PB_ERR_UNSUPPORTED). */
+ * periodic = 0: open boundaries as the reference's non-periodic branch --
+ * cells of edge rmax, one past each top face, no neighbour across a face
+ * (UINT_MAX in the neighbour table), no image in the forces, and steps do
+ * not wrap positions (pb_md_wrap still does on request).  Open boxes run on
+ * the full-shell cell-list force only: with PB_MD_HALF_SHELL or a neighbour
+ * list the call returns PB_ERR_UNSUPPORTED. */
 int pb_md_setup_cells(pb_md *h, float rmax, int periodic);
 /* Grid of the last setup: cells per axis and cell edge (blocknum, blocklen). */
 int pb_md_grid(const pb_md *h, uint32_t n3[3], float len3[3], uint32_t *ncells);

@@ -36,15 +36,21 @@ struct Grid {
   uint32_t ncells;
 };
 
-// cudaCutoffBlock::setupCutoffBlock, periodic branch (cudaCutoffBlock.cu:97-113):
-// blocknum = (uint32)(c / rmax), blocklen = c / (float)blocknum, all in FP32.
-int make_grid(const float *cell6, float rmax, Grid &g) {
+// cudaCutoffBlock::setupCutoffBlock (cudaCutoffBlock.cu:97-113), all in FP32.
+// Periodic: blocknum = (uint32)(c / rmax), blocklen = c / (float)blocknum.
+// Open: blocklen = rmax, blocknum = (uint32)(c / rmax) + 1.
+int make_grid(const float *cell6, float rmax, Grid &g, int periodic = 1) {
   for (int i = 0; i < 3; ++i) {
     const float c = cell6[2 * i + 1] - cell6[2 * i];
     const float q = c / rmax;
-    if (!(q >= 3.0f)) return -1;  // reference asserts blocknum > 2
-    g.n[i] = static_cast<uint32_t>(q);
-    g.len[i] = c / static_cast<float>(g.n[i]);
+    if (periodic) {
+      g.n[i] = static_cast<uint32_t>(q);
+      g.len[i] = c / static_cast<float>(g.n[i]);
+    } else {
+      g.n[i] = static_cast<uint32_t>(q) + 1u;
+      g.len[i] = rmax;
+    }
+    if (!(q >= 0.0f) || g.n[i] <= 2) return -1;  // reference asserts blocknum > 2
     g.lo[i] = cell6[2 * i];
   }
   g.ncells = g.n[0] * g.n[1] * g.n[2];
@@ -388,9 +394,17 @@ extern "C" {
 
 // ---- stateless helpers -------------------------------------------------------
 
+int orc_grid_p(const float *cell6, float rc, int periodic, uint32_t *n3, float *len3);
+int orc_bin_p(const float *r4, uint32_t N, const float *cell6, float rc, int periodic,
+              uint32_t *cid);
+
 int orc_grid(const float *cell6, float rc, uint32_t *n3, float *len3) {
+  return orc_grid_p(cell6, rc, 1, n3, len3);
+}
+
+int orc_grid_p(const float *cell6, float rc, int periodic, uint32_t *n3, float *len3) {
   Grid g;
-  if (make_grid(cell6, rc, g)) return -1;
+  if (make_grid(cell6, rc, g, periodic)) return -1;
   for (int k = 0; k < 3; ++k) {
     n3[k] = g.n[k];
     len3[k] = g.len[k];
@@ -400,14 +414,19 @@ int orc_grid(const float *cell6, float rc, uint32_t *n3, float *len3) {
 
 int orc_neighbor_table(const float *cell6, float rc, int periodic, uint32_t *out) {
   Grid g;
-  if (make_grid(cell6, rc, g)) return -1;
+  if (make_grid(cell6, rc, g, periodic)) return -1;
   neighbor_table(g, periodic, out);
   return 0;
 }
 
 int orc_bin(const float *r4, uint32_t N, const float *cell6, float rc, uint32_t *cid) {
+  return orc_bin_p(r4, N, cell6, rc, 1, cid);
+}
+
+int orc_bin_p(const float *r4, uint32_t N, const float *cell6, float rc, int periodic,
+              uint32_t *cid) {
   Grid g;
-  if (make_grid(cell6, rc, g)) return -1;
+  if (make_grid(cell6, rc, g, periodic)) return -1;
 #pragma omp parallel for schedule(static)
   for (long i = 0; i < (long)N; ++i) cid[i] = cell_of(g, r4[4 * i], r4[4 * i + 1], r4[4 * i + 2]);
   return 0;

@@ -58,6 +58,8 @@ def lib() -> C.CDLL:
     if _lib is None:
         L = _load(LIB_ORACLE)
         L.orc_grid.argtypes = [_f32p, C.c_float, _u32p, _f32p]
+        L.orc_grid_p.argtypes = [_f32p, C.c_float, C.c_int, _u32p, _f32p]
+        L.orc_bin_p.argtypes = [_f32p, C.c_uint32, _f32p, C.c_float, C.c_int, _u32p]
         L.orc_neighbor_table.argtypes = [_f32p, C.c_float, C.c_int, _u32p]
         L.orc_bin.argtypes = [_f32p, C.c_uint32, _f32p, C.c_float, _u32p]
         L.orc_cell_list.argtypes = [_u32p, C.c_void_p, C.c_uint32, C.c_uint32, _u32p, _u32p]
@@ -107,6 +109,8 @@ def ref() -> C.CDLL:
         L.ref_set_positions.argtypes = [C.c_void_p, _f32p]
         L.ref_setup_cells.argtypes = [C.c_void_p, C.c_float]
         L.ref_setup_cells.restype = C.c_int
+        L.ref_setup_cells_p.argtypes = [C.c_void_p, C.c_float, C.c_int]
+        L.ref_setup_cells_p.restype = C.c_int
         for n in ("ref_calc_block_id", "ref_calc_force", "ref_clear_force", "ref_wrap"):
             getattr(L, n).argtypes = [C.c_void_p]
         L.ref_calc_mv2.argtypes = [C.c_void_p]
@@ -150,25 +154,25 @@ def _cell6(box) -> np.ndarray:
 # ---------------------------------------------------------------- stateless
 
 
-def grid(box, rc):
+def grid(box, rc, periodic=True):
     n = np.zeros(3, np.uint32)
     ln = np.zeros(3, np.float32)
-    if lib().orc_grid(_cell6(box), rc, n, ln):
+    if lib().orc_grid_p(_cell6(box), rc, int(periodic), n, ln):
         raise ValueError("cell grid needs at least 3 cells per dimension")
     return n, ln
 
 
 def neighbor_table(box, rc, periodic=True):
-    n, _ = grid(box, rc)
+    n, _ = grid(box, rc, periodic)
     out = np.zeros(int(np.prod(n)) * 27, np.uint32)
     lib().orc_neighbor_table(_cell6(box), rc, int(periodic), out)
     return out.reshape(-1, 27)
 
 
-def bin_cells(r4, box, rc):
+def bin_cells(r4, box, rc, periodic=True):
     r4 = np.ascontiguousarray(r4, np.float32).reshape(-1, 4)
     out = np.zeros(len(r4), np.uint32)
-    if lib().orc_bin(r4.reshape(-1), len(r4), _cell6(box), rc, out):
+    if lib().orc_bin_p(r4.reshape(-1), len(r4), _cell6(box), rc, int(periodic), out):
         raise ValueError("bad grid")
     return out
 
@@ -283,7 +287,7 @@ class RefKernels:
     """The reference's own MD kernels run on the CPU (oracle/_ref)."""
 
     def __init__(self, box, rc, r, v, mass, types, lj_sigma_eps, ntypes=1,
-                 gaussian=False, rmax2=None, kB=1.0, tol=1e-8):
+                 gaussian=False, rmax2=None, kB=1.0, tol=1e-8, periodic=True):
         L = ref()
         self.N = len(r)
         self.h = L.ref_create(self.N, _cell6(box), int(gaussian))
@@ -295,7 +299,7 @@ class RefKernels:
                      np.ascontiguousarray(v, np.float64)[:, :3].copy().reshape(-1),
                      np.ascontiguousarray(mass, np.float64),
                      np.ascontiguousarray(types, np.uint32))
-        if L.ref_setup_cells(self.h, rc):
+        if L.ref_setup_cells_p(self.h, rc, int(periodic)):
             raise ValueError("reference grid needs blocknum > 2")
         L.ref_clear_force(self.h)
 

@@ -173,9 +173,10 @@ void ref_set_positions(void *h, const float *r4) {
   std::memcpy(s.r.data(), r4, sizeof(float4) * s.N);
 }
 
-// cudaCutoffBlock::setupCutoffBlock (cudaCutoffBlock.cu:75-231), periodic,
-// many-particle blocks.
-int ref_setup_cells(void *h, float rmax) {
+// cudaCutoffBlock::setupCutoffBlock (cudaCutoffBlock.cu:75-231), many-particle
+// blocks; periodic, or open (one block of length rmax past each top face, no
+// wrapped neighbours).
+int ref_setup_cells_p(void *h, float rmax, int periodic) {
   RefSys &s = *(RefSys *)h;
   s.blocklen.assign(6, 0);
   s.blocknum.assign(3, 0);
@@ -185,8 +186,13 @@ int ref_setup_cells(void *h, float rmax) {
   real c[3];
   for (int i = 0; i < 3; ++i) {
     c[i] = s.cell[i * 2 + 1] - s.cell[i * 2];
-    s.blocknum[i] = static_cast<uint32_t>(c[i] / rmax);
-    s.blocklen[i] = c[i] / static_cast<real>(s.blocknum[i]);
+    if (periodic) {
+      s.blocknum[i] = static_cast<uint32_t>(c[i] / rmax);
+      s.blocklen[i] = c[i] / static_cast<real>(s.blocknum[i]);
+    } else {
+      s.blocklen[i] = rmax;
+      s.blocknum[i] = static_cast<uint32_t>(c[i] / rmax) + 1;
+    }
     if (s.blocknum[i] <= 2) return -1;
     s.blocklen[i + 3] = s.cell[i * 2];
   }
@@ -194,7 +200,7 @@ int ref_setup_cells(void *h, float rmax) {
   s.bindex.assign(s.totalNumBlock + 1, 0);
   s.bindex[s.totalNumBlock] = s.N;
   s.blockNeighbor.assign((size_t)s.totalNumBlock * 27, 0);
-  launch(dim3(s.MPnum), true, calc_BlockNeighbor, s.blockNeighbor.data(), 1, true, 27,
+  launch(dim3(s.MPnum), true, calc_BlockNeighbor, s.blockNeighbor.data(), 1, periodic != 0, 27,
          s.blocknum[0], s.blocknum[1], s.blocknum[2]);
   s.tmp81N.assign((size_t)s.N * 81, 0);
   s.THnum2D2 = s.THnum2D;
@@ -204,6 +210,8 @@ int ref_setup_cells(void *h, float rmax) {
   }
   return 0;
 }
+
+int ref_setup_cells(void *h, float rmax) { return ref_setup_cells_p(h, rmax, 1); }
 
 // cudaCutoffBlock::calcBlockID + cudaSortedPositions::calcBlockID
 void ref_calc_block_id(void *h) {

@@ -8,6 +8,9 @@ namespace pb {
 
 constexpr int kMaxTypes = 8;
 constexpr uint32_t kNone = 0xffffffffu;
+// Neighbour cell or column outside an open box (the reference's UINT_MAX in
+// its block-neighbour table).
+constexpr uint32_t kNoCell = 0xffffffffu;
 
 // Device status bits, OR-ed into a per-system status word.  No kernel traps;
 // the host reads the word and turns it into a pb_status.
@@ -29,6 +32,7 @@ struct Grid {
   float lo[3];       // box minimum corner (cellmin)
   float L[3];        // box lengths (xmax - xmin etc., FP32)
   uint32_t ncells;
+  int periodic;      // 0: open boundaries (no images, no wrap)
 };
 
 // Lennard-Jones parameters per ordered type pair, row-major [ti * nt + tj].

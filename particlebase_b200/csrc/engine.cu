@@ -91,9 +91,9 @@ namespace {
 // Column ranking and force work items depend only on the grid and the z-run
 // length; batches of many similar systems share them.
 struct PlanKey {
-  int nx, ny, nz, seg;
+  int nx, ny, nz, seg, periodic;
   bool operator<(const PlanKey &o) const {
-    return std::tie(nx, ny, nz, seg) < std::tie(o.nx, o.ny, o.nz, o.seg);
+    return std::tie(nx, ny, nz, seg, periodic) < std::tie(o.nx, o.ny, o.nz, o.seg, o.periodic);
   }
 };
 struct Plan {
@@ -104,7 +104,7 @@ struct Plan {
 std::shared_ptr<const Plan> cached_plan(const Grid &g, int seg) {
   static std::mutex mu;
   static std::map<PlanKey, std::shared_ptr<const Plan>> cache;
-  const PlanKey k{g.n[0], g.n[1], g.n[2], seg};
+  const PlanKey k{g.n[0], g.n[1], g.n[2], seg, g.periodic};
   {
     std::lock_guard<std::mutex> lk(mu);
     auto it = cache.find(k);
@@ -530,8 +530,11 @@ int engine_setup_cells(Engine &e) {
     SysParams &P = e.sp[s];
     if (!P.cell_set) return fail(e, PB_ERR_STATE, "set the cell first");
     Grid g;
-    if (!make_grid(P.cell, P.rmax, g))
+    if (!make_grid(P.cell, P.rmax, g, P.periodic))
       return fail(e, PB_ERR_ARG, "cell grid needs at least 3 cells per axis (blocknum > 2)");
+    if (!P.periodic && ((e.flags & PB_MD_HALF_SHELL) || e.nl_on))
+      return fail(e, PB_ERR_UNSUPPORTED,
+                  "open boundaries run on the full-shell cell-list force only");
     P.grid = g;
     const double apc = (double)P.n / g.ncells;
     apc_max = std::max(apc_max, apc);
@@ -557,7 +560,8 @@ int engine_setup_cells(Engine &e) {
     e.item0[s] = (uint32_t)items.size();
     for (ForceItem it : plan.items) {  // the system's items: its index and first cell key
       it.sys = s;
-      for (auto &k : it.kbase) k += (uint32_t)ncells;
+      for (auto &k : it.kbase)
+        if (k != kNoCell) k += (uint32_t)ncells;
       items.push_back(it);
     }
     P.key_of_ref.clear();
@@ -665,7 +669,10 @@ IntegrateArgs engine_iargs(Engine &e, int wrap) {
   a.sys = e.d_sysint;
   a.map = e.d_map;
   a.nblocks = e.nblocks;
-  a.wrap = wrap;
+  // an open box is never wrapped by a step (pb_md_wrap still wraps on request)
+  bool open_box = false;
+  for (const auto &P : e.sp) open_box = open_box || !P.periodic;
+  a.wrap = wrap && !open_box;
   a.sc = e.sc;
   a.partials = e.ipartials;
   a.status = e.status;
@@ -754,6 +761,8 @@ int engine_use_nlist(Engine &e, float thickness) {
     return PB_OK;
   }
   if (!(thickness < 1e30f)) return fail(e, PB_ERR_ARG, "bad thickness");
+  if (!e.sp[0].periodic)
+    return fail(e, PB_ERR_UNSUPPORTED, "the neighbour list needs a periodic box");
   e.nl_on = true;
   e.nl_skin = thickness;
   e.nl_built = false;

@@ -26,6 +26,7 @@ struct SysParams {
   double m0 = 1.0;
   float dt = 0.005f;
   bool r_set = false;     // positions imported or set (the cell build may be timed)
+  bool periodic = true;   // false: open boundaries (pb_md_setup_cells(periodic = 0))
   std::vector<uint32_t> key_of_ref, ref_of_key;  // reference cell id <-> packed key - cell0
 };
 

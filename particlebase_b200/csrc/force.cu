@@ -79,6 +79,7 @@ struct ItemDesc {
   float sz_lo, sz_mid, sz_hi;  // frame shift of staged cell 0, 1..nseg, nseg + 1
   uint32_t item, sys, home_g0, hb, H, nclus, ntask, sentinel, base;
   int z0, nz, nseg;
+  int periodic;        // 0: open box (neighbour columns may be absent, no z images)
   int skip;            // the system's step budget is spent
   int overflow;        // the stage exceeds the capacity: global-memory path
   LJLocal<NT> lj;
@@ -308,6 +309,7 @@ __device__ bool produce_item(const ForceBufs &b, uint32_t item, ItemDesc<NT> &d,
   const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
   const int z0 = it.z0, z1 = it.z1, nseg = z1 - z0;
   const int ncell = nseg + 2;  // staged cells per column
+  const bool per = g.periodic != 0;
   for (int t = pt; t < NT * NT; t += kPT) {
     const LJTable &Tb = b.lj[S.lj];
     const int a = t / NT, c = t % NT;
@@ -325,17 +327,18 @@ __device__ bool produce_item(const ForceBufs &b, uint32_t item, ItemDesc<NT> &d,
     const int wx = ax < 0 ? -1 : (ax >= nx ? 1 : 0);
     const int wy = ay < 0 ? -1 : (ay >= ny ? 1 : 0);
     // frame: F = L on the top face; staged = x + w L - F, so the shift is F - w L
-    const float Fx = cx == nx - 1 ? g.L[0] : 0.0f, Fy = cy == ny - 1 ? g.L[1] : 0.0f;
-    d.sx[c] = Fx - (float)wx * g.L[0];
-    d.sy[c] = Fy - (float)wy * g.L[1];
+    // (an open box has no images and no frame shift)
+    const float Fx = per && cx == nx - 1 ? g.L[0] : 0.0f, Fy = per && cy == ny - 1 ? g.L[1] : 0.0f;
+    d.sx[c] = per ? Fx - (float)wx * g.L[0] : 0.0f;
+    d.sy[c] = per ? Fy - (float)wy * g.L[1] : 0.0f;
     d.kbase[c] = it.kbase[c];
   }
   // an item on the top face works in the frame shifted down by L, where the
   // shifts of its atoms (all in the upper half) are exact; a whole column
   // keeps the unshifted frame and rounds only the image above its top
-  const float Fz = z1 == nz && z0 > 0 ? g.L[2] : 0.0f;
-  const float sz_lo = z0 == 0 ? Fz + g.L[2] : Fz;  // image z0 - 1 wraps below when z0 == 0
-  const float sz_hi = z1 == nz ? Fz - g.L[2] : Fz;  // image z1 wraps above when z1 == nz
+  const float Fz = per && z1 == nz && z0 > 0 ? g.L[2] : 0.0f;
+  const float sz_lo = per && z0 == 0 ? Fz + g.L[2] : Fz;  // image z0 - 1 wraps below when z0 == 0
+  const float sz_hi = per && z1 == nz ? Fz - g.L[2] : Fz;  // image z1 wraps above when z1 == nz
   if (pt == 0) {
     d.sz_lo = sz_lo;
     d.sz_mid = Fz;
@@ -343,17 +346,23 @@ __device__ bool produce_item(const ForceBufs &b, uint32_t item, ItemDesc<NT> &d,
     d.z0 = z0;
     d.nz = nz;
     d.nseg = nseg;
+    d.periodic = per;
     d.lj.sc_rc = b.sc_rc;
     d.lj.sc_f0 = b.sc_f0;
   }
-  // cell starts and counts of the 9 x ncell staged cells
+  // cell starts and counts of the 9 x ncell staged cells; in an open box a
+  // column past a face, or a cell past the bottom or top, is empty
   for (int t = pt; t < 9 * ncell; t += kPT) {
     const int c = t / ncell, k = t % ncell;
-    const int zc = (z0 - 1 + k + nz) % nz;
-    const uint32_t key = it.kbase[c] + (uint32_t)zc;
-    const uint32_t s0 = b.start[key];
+    const int zr = z0 - 1 + k, zc = (zr + nz) % nz;
+    uint32_t s0 = 0, s1 = 0;
+    if (per || (it.kbase[c] != kNoCell && zr >= 0 && zr < nz)) {
+      const uint32_t key = it.kbase[c] + (uint32_t)zc;
+      s0 = b.start[key];
+      s1 = b.start[key + 1];
+    }
     sc.gstart[c][k] = s0;
-    sc.cnt[c][k] = b.start[key + 1] - s0;
+    sc.cnt[c][k] = s1 - s0;
   }
   producer_sync<kProd>();
   // exclusive prefix over the cells of each column, one warp per column
@@ -893,8 +902,10 @@ __device__ void consume_task_global(const ForceBufs &b, const ItemDesc<NT> &d, u
     const int ti = NT == 1 ? 0 : __float_as_int(p.w);
     PairAcc<NT, ENERGY, Acc, MODE> acc;
     for (int c = 0; c < 9; ++c) {
+      if (!d.periodic && d.kbase[c] == kNoCell) continue;  // no column past an open face
       for (int k = kmin - 1; k <= kmax + 1; ++k) {
-        const int zc = (z0 - 1 + k + nz) % nz;
+        const int zr = z0 - 1 + k, zc = (zr + nz) % nz;
+        if (!d.periodic && (zr < 0 || zr >= nz)) continue;
         const uint32_t key = d.kbase[c] + (uint32_t)zc;
         const float sz = k == 0 ? d.sz_lo : (k == nseg + 1 ? d.sz_hi : d.sz_mid);
         if (c == 4)

@@ -169,9 +169,9 @@ int pb_md_import(pb_md *h, const pb_particle *p, uint32_t n) {
 
 int pb_md_setup_cells(pb_md *h, float rmax, int periodic) {
   if (!h || !(rmax > 0)) return PB_ERR_ARG;
-  if (!periodic) return fail(h, PB_ERR_UNSUPPORTED, "only periodic boxes are supported");
   if (!h->p().cell_set) return fail(h, PB_ERR_STATE, "set the cell first");
   h->p().rmax = rmax;
+  h->p().periodic = periodic != 0;
   return engine_setup_cells(h->e);
 }
 

@@ -6,16 +6,23 @@
 
 namespace pb {
 
-bool make_grid(const float cell6[6], float rmax, Grid &g) {
+bool make_grid(const float cell6[6], float rmax, Grid &g, bool periodic) {
   for (int i = 0; i < 3; ++i) {
     const float c = cell6[2 * i + 1] - cell6[2 * i];
     const float q = c / rmax;
-    if (!(q >= 3.0f) || q > 1.0e6f) return false;
-    g.n[i] = static_cast<int>(static_cast<uint32_t>(q));
-    g.len[i] = c / static_cast<float>(static_cast<uint32_t>(g.n[i]));
+    if (periodic) {
+      if (!(q >= 3.0f) || q > 1.0e6f) return false;
+      g.n[i] = static_cast<int>(static_cast<uint32_t>(q));
+      g.len[i] = c / static_cast<float>(static_cast<uint32_t>(g.n[i]));
+    } else {
+      if (!(q >= 2.0f) || q > 1.0e6f) return false;
+      g.n[i] = static_cast<int>(static_cast<uint32_t>(q) + 1u);
+      g.len[i] = rmax;
+    }
     g.lo[i] = cell6[2 * i];
     g.L[i] = c;
   }
+  g.periodic = periodic ? 1 : 0;
   const uint64_t nc = (uint64_t)g.n[0] * g.n[1] * g.n[2];
   if (nc >= 0xffffffffull) return false;
   g.ncells = (uint32_t)nc;
@@ -60,8 +67,11 @@ void neighbor_table(const Grid &g, std::vector<uint32_t> &out) {
         for (int a = -1; a <= 1; ++a)
           for (int b = -1; b <= 1; ++b)
             for (int c = -1; c <= 1; ++c) {
+              const bool inside = i + a >= 0 && i + a < nx && j + b >= 0 && j + b < ny &&
+                                  k + c >= 0 && k + c < nz;
               const long i2 = (i + a + nx) % nx, j2 = (j + b + ny) % ny, k2 = (k + c + nz) % nz;
-              out[I * 27 + L++] = (uint32_t)(k2 + j2 * nz + i2 * nz * ny);
+              out[I * 27 + L++] = g.periodic || inside ? (uint32_t)(k2 + j2 * nz + i2 * nz * ny)
+                                                       : kNoCell;
             }
       }
 }
@@ -144,8 +154,12 @@ void append_items(uint32_t sys, const Grid &g, int seg, uint32_t cell0,
     it.cx = (uint16_t)cx;
     it.cy = (uint16_t)cy;
     for (int k = 0; k < 9; ++k) {
-      const int ax = (cx + k / 3 - 1 + nx) % nx, ay = (cy + k % 3 - 1 + ny) % ny;
-      it.kbase[k] = cell0 + rank[(size_t)ax * ny + ay] * (uint32_t)nz;
+      const int ax0 = cx + k / 3 - 1, ay0 = cy + k % 3 - 1;
+      const int ax = (ax0 + nx) % nx, ay = (ay0 + ny) % ny;
+      const bool inside = ax0 >= 0 && ax0 < nx && ay0 >= 0 && ay0 < ny;
+      // an open box has no column past its faces
+      it.kbase[k] = g.periodic || inside ? cell0 + rank[(size_t)ax * ny + ay] * (uint32_t)nz
+                                         : kNoCell;
     }
     int z = 0;
     for (int p = 0; p < parts; ++p) {

@@ -10,18 +10,20 @@
 
 namespace pb {
 
-// cudaCutoffBlock::setupCutoffBlock, periodic branch (cudaCutoffBlock.cu:97-113),
-// in the same FP32 operations: blocknum = (uint32)(c / rmax),
-// blocklen = c / (float)blocknum.  Returns false if any axis has < 3 cells
-// (the reference asserts blocknum > 2).
-bool make_grid(const float cell6[6], float rmax, Grid &g);
+// cudaCutoffBlock::setupCutoffBlock (cudaCutoffBlock.cu:97-113) in the same
+// FP32 operations.  Periodic: blocknum = (uint32)(c / rmax),
+// blocklen = c / (float)blocknum.  Open boundaries: blocklen = rmax and
+// blocknum = (uint32)(c / rmax) + 1, one block past the top face.  Returns
+// false if any axis has < 3 cells (the reference asserts blocknum > 2).
+bool make_grid(const float cell6[6], float rmax, Grid &g, bool periodic = true);
 
 // rank[d0 * ny + d1] = position of column (d0, d1) along a Z-order curve;
 // xy[rank] = d0 * ny + d1.
 void morton_columns(int nx, int ny, std::vector<uint32_t> &rank, std::vector<uint32_t> &xy);
 
-// Reference 27-neighbour table (calc_BlockNeighbor, cudaCutoffBlock.cu:17-65),
-// periodic, in reference cell numbering d2 + d1 nz + d0 nz ny.
+// Reference 27-neighbour table (calc_BlockNeighbor, cudaCutoffBlock.cu:17-65)
+// in reference cell numbering d2 + d1 nz + d0 nz ny; in an open box a
+// neighbour outside the grid is kNoCell.
 void neighbor_table(const Grid &g, std::vector<uint32_t> &out);
 
 // z cells per force work item for a mean cell occupancy: about 200 * scale

@@ -7,7 +7,8 @@ calc_BlockNeighbor, calcF_IJpairWithBlock_F4<MDpairForce<potentialLJ>> +
 reduce27_F4, propagateVelocityVerlet_F4, the Gaussian-thermostat kernels,
 applyPeriodicCondition_F4, adjustVelocity_F4 / adjustVelocity_VD, mulArray
 (scaleTemp), MDpairForce<potentialSC>, correctConstTemp_F4, calcA_F4 and
-propagateEuler_F4 of initialAnnealing) -- on small seeded inputs and stores the outputs in
+propagateEuler_F4 of initialAnnealing; the open-box grid and block neighbours of
+setupCutoffBlock(rmax, false)) -- on small seeded inputs and stores the outputs in
 tests/golden/*.npz.  The oracle is checked against these files in
 tests/test_oracle.py, so the pin holds where the reference checkout is absent.
 
@@ -198,6 +199,31 @@ def main() -> None:
     out["anneal_args"] = np.array([5, 0.005, 1.2, 1.0, 0.72], np.float64)
     out["anneal_r4"] = Rn.get4("r")
     out["anneal_v4"] = Rn.get4("v")
+
+    # 13. open boundaries (setupCutoffBlock(rmax, periodic = false)): a jittered
+    # simple-cubic gas in a 20-sigma box, plus atoms in the extra block past
+    # the top faces and just below the bottom ones (clamped to cell 0).
+    rng = np.random.default_rng(13)
+    g = (np.arange(12) + 0.5) * (20.0 / 12)
+    ro = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    ro = ro + rng.uniform(-0.2, 0.2, ro.shape)
+    extra = np.array([[20.6, 10.0, 10.0], [10.0, 21.2, 5.0], [3.0, 3.0, 21.9],
+                      [-0.05, 12.0, 12.0], [21.5, 21.5, 21.5]])
+    ro = np.concatenate([ro, extra]).astype(np.float32).astype(np.float64)
+    so = W.LJSystem(box=np.array([0, 20, 0, 20, 0, 20], np.float32), r=ro,
+                    v=np.zeros_like(ro), mass=np.ones(len(ro)),
+                    types=np.zeros(len(ro), np.uint32), lj=W.single_type_lj(), rc=2.5)
+    Ro = po.RefKernels(so.box, so.rc, ro, so.v, so.mass, so.types, [1.0, 1.0], periodic=False)
+    Ro.calc_block_id()
+    bid, pid, _ = Ro.cells()
+    cell_of = np.empty(so.n, np.uint32)
+    cell_of[pid] = bid
+    Ro.calc_force()
+    out["open_r4"] = Ro.get4("r")
+    out["open_grid"] = Ro.grid()[0]
+    out["open_cell_of"] = cell_of
+    out["open_neighbors"] = Ro.neighbors()
+    out["open_F"] = Ro.get4("F")
 
     path = os.path.join(HERE, "reference_kernels.npz")
     np.savez_compressed(path, **out)

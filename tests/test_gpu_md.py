@@ -325,6 +325,54 @@ def test_two_atoms_analytic_and_across_faces(cuda_lib):
                 assert F[1, axis] == pytest.approx(-f, rel=2e-5, abs=2e-4)
 
 
+@pytest.mark.parametrize("fp64_sums", [False, True])
+def test_open_box_vs_reference_kernels(cuda_lib, golden, fp64_sums):
+    """setupCutoffBlock(rmax, periodic = false) against the reference's kernels
+    on the same input (golden): the grid with one block past each top face,
+    every atom's cell (atoms past the top faces and below the bottom ones
+    included), the neighbour table with UINT_MAX outside, and the forces, which
+    take no image across a face; a step leaves positions unwrapped."""
+    r4 = golden["open_r4"]
+    r = r4[:, :3].astype(np.float64)
+    box = np.array([0, 20, 0, 20, 0, 20], np.float32)
+    s = W.LJSystem(box=box, r=r, v=np.zeros_like(r), mass=np.ones(len(r)),
+                   types=np.zeros(len(r), np.uint32), lj=W.single_type_lj(), rc=2.5)
+    p = md(cuda_lib, s, fp64_forces=fp64_sums)
+    p.setupCutoffBlock(2.5, periodic=False)
+    n3, ln, C = p.grid()
+    assert np.array_equal(n3, golden["open_grid"]) and np.all(ln == np.float32(2.5))
+    p.calcBlockID()
+    assert np.array_equal(p.get("cell_of"), golden["open_cell_of"])
+    assert np.array_equal(p.get("neighbors"), golden["open_neighbors"])
+    p.calcForce()
+    F = p.get("F")[:, :3].astype(np.float64)
+    assert relrms(F, golden["open_F"][:, :3].astype(np.float64)) < FORCE_RELRMS
+    # one velocity-Verlet step: the atoms past the top faces stay there
+    p.clearForce()
+    p.run(0.001, 1)
+    r_after = p.get("r")[:, :3]
+    assert r_after[-1].min() > 20.0 and r_after[-2][0] < 0.0
+    assert p.status() == 0
+    p.close()
+
+
+def test_open_box_rejects_half_shell_and_lists(cuda_lib, golden):
+    r = golden["open_r4"][:, :3].astype(np.float64)
+    s = W.LJSystem(box=np.array([0, 20, 0, 20, 0, 20], np.float32), r=r, v=np.zeros_like(r),
+                   mass=np.ones(len(r)), types=np.zeros(len(r), np.uint32),
+                   lj=W.single_type_lj(), rc=2.5)
+    from particlebase_b200._lib import PBError
+    p = md(cuda_lib, s, half_shell=True)
+    with pytest.raises(PBError):
+        p.setupCutoffBlock(2.5, periodic=False)
+    p.close()
+    q = md(cuda_lib, s)
+    q.setupCutoffBlock(2.5, periodic=False)
+    with pytest.raises(PBError):
+        q.useNList(0.3)
+    q.close()
+
+
 def test_empty_cells_and_crowded_cells(cuda_lib, po):
     """Sparse gas with many empty cells plus a clump of 60 atoms in one cell:
     exercises empty ranges, the >32-member cell ordering and the global-memory
@@ -384,8 +432,12 @@ def test_errors_are_returned_not_fatal(cuda_lib):
     with pytest.raises(L.PBError) as e:
         p.setupCutoffBlock(2.5)  # 2 cells per axis: the reference asserts blocknum > 2
     assert e.value.code == 1
-    with pytest.raises(L.PBError):
-        p.setupCutoffBlock(1.0, periodic=False)
+    # an open box has one cell past each top face: 5 / 3 -> 1 + 1 = 2 cells, too few
+    with pytest.raises(L.PBError) as e:
+        p.setupCutoffBlock(3.0, periodic=False)
+    assert e.value.code == 1
+    p.setupCutoffBlock(2.5, periodic=False)  # 2 + 1 = 3 cells per axis
+    assert list(p.grid()[0]) == [3, 3, 3]
 
 
 def test_minimize_matches_oracle(cuda_lib, po):

@@ -36,6 +36,42 @@ def test_neighbor_table_matches_reference(po, golden):
     assert np.array_equal(po.neighbor_table(golden["c1_box"], 2.5), golden["c1_neighbors"])
 
 
+OPEN_BOX = np.array([0, 20, 0, 20, 0, 20], np.float32)
+
+
+def open_box_direct_forces(r4, rc=2.5):
+    """Truncated LJ (sigma = eps = 1) summed over all pairs, no images (FP64)."""
+    r = r4[:, :3].astype(np.float64)
+    F = np.zeros_like(r)
+    for i in range(len(r)):
+        d = r[i] - r
+        r2 = (d * d).sum(1)
+        m = (r2 < rc * rc) & (r2 > 0)
+        inv2 = 1.0 / r2[m]
+        s6 = inv2 ** 3
+        F[i] = ((24.0 * s6 * (2.0 * s6 - 1.0) * inv2)[:, None] * d[m]).sum(0)
+    return F
+
+
+def test_open_box_cells_match_reference(po, golden):
+    """setupCutoffBlock(rmax, periodic = false): one block of length rmax past
+    each top face, no wrapped neighbours (UINT_MAX), and the same clamps."""
+    n, ln = po.grid(OPEN_BOX, 2.5, periodic=False)
+    assert np.array_equal(n, golden["open_grid"])
+    assert np.all(ln == np.float32(2.5))
+    assert np.array_equal(po.bin_cells(golden["open_r4"], OPEN_BOX, 2.5, periodic=False),
+                          golden["open_cell_of"])
+    assert np.array_equal(po.neighbor_table(OPEN_BOX, 2.5, periodic=False),
+                          golden["open_neighbors"])
+
+
+def test_open_box_forces_match_reference(golden):
+    """The reference's force kernels on the open box equal the all-pairs sum
+    without images (the pins the GPU's open-box forces are checked against)."""
+    F = open_box_direct_forces(golden["open_r4"])
+    assert relrms(golden["open_F"][:, :3].astype(np.float64), F) < 1e-6
+
+
 def test_cell_list_is_stable_counting_sort(po):
     rng = np.random.default_rng(0)
     cid = rng.integers(0, 50, 1000).astype(np.uint32)
