@@ -387,6 +387,14 @@ int pb_batch_estimate_bytes(const uint32_t *natoms, const float *cells6, const f
  * count, with the result it would have alone (bit for bit, same flags). */
 typedef struct pb_srv pb_srv;
 
+/* The library's device memory pool: every handle allocates from it, and it
+   keeps the memory they free.  Growing it maps new pages, which inside a busy
+   process took up to a second per growth.  pb_pool_reserve takes `bytes` into
+   it at once (PB_ERR_OOM when they are not free); pb_pool_trim hands its unused
+   memory back to the device.  No counterpart in the reference. */
+int pb_pool_reserve(size_t bytes);
+int pb_pool_trim(void);
+
 typedef struct pb_srv_config {
   size_t hbm_budget;      /* bytes the resident batch may hold (estimate); 0 = 90% of free */
   uint64_t max_atoms;     /* resident atom cap (0 = none): bounds the step time */
@@ -396,6 +404,11 @@ typedef struct pb_srv_config {
   int mode;               /* PB_MODE_VV or PB_MODE_GAUSS */
   int force_threads;      /* 0 = default (256) */
   float seg_scale;        /* 0 = 1.0 */
+  size_t reserve_bytes;   /* device memory taken into the library's pool at creation
+                             (pb_pool_reserve) and handed back by pb_srv_destroy, so
+                             that repacks never wait for the pool to grow; 0 = none,
+                             SIZE_MAX = the whole HBM budget.  Not available: the
+                             server runs without it. */
 } pb_srv_config;
 
 typedef struct pb_srv_job {

@@ -47,7 +47,8 @@ class pb_particle(C.Structure):
 class pb_srv_config(C.Structure):
     _fields_ = [("hbm_budget", C.c_size_t), ("max_atoms", C.c_uint64), ("max_jobs", C.c_uint32),
                 ("chunk_ms", C.c_float), ("flags", C.c_uint32), ("mode", C.c_int),
-                ("force_threads", C.c_int), ("seg_scale", C.c_float)]
+                ("force_threads", C.c_int), ("seg_scale", C.c_float),
+                ("reserve_bytes", C.c_size_t)]
 
 
 class pb_srv_job(C.Structure):
@@ -165,6 +166,8 @@ def _declare(L: C.CDLL) -> None:
         "pb_srv_result": [vp, C.c_uint64, vp, vp, C.c_size_t, vp],
         "pb_srv_release": [vp, C.c_uint64],
         "pb_srv_stats_get": [vp, C.POINTER(pb_srv_stats)],
+        "pb_pool_reserve": [C.c_size_t],
+        "pb_pool_trim": [],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

@@ -141,6 +141,10 @@ int engine_step(Engine &e, int mode);
 // Device scratch from the engine's pool, on its stream (stream-ordered).
 cudaError_t engine_alloc_bytes(Engine &e, void **p, size_t bytes);
 void engine_free_bytes(Engine &e, void *p);
+// The device pool engines allocate from: reserve takes `bytes` into it at once
+// (PB_ERR_OOM when they are not free); trim hands its unused memory back.
+int engine_pool_reserve(size_t bytes);
+void engine_pool_trim();
 // Neighbour list: thickness >= 0 turns it on (rows within rc + thickness),
 // thickness < 0 off; make rebuilds the cell list and the neighbour list.
 int engine_use_nlist(Engine &e, float thickness);

@@ -461,4 +461,11 @@ int pb_md_set(pb_md *h, int field, const void *host, size_t bytes) {
   return PB_OK;
 }
 
+int pb_pool_reserve(size_t bytes) { return engine_pool_reserve(bytes); }
+
+int pb_pool_trim(void) {
+  engine_pool_trim();
+  return PB_OK;
+}
+
 }  // extern "C"

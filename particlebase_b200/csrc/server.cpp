@@ -80,6 +80,7 @@ struct pb_srv {
   double ms_per_atom_step = 5e-7;
   double last_repack_ms = 0.0;
   bool trace = false;  // PB_SRV_TRACE: per-repack phase times on stderr
+  bool reserved = false;  // the pool took reserve_bytes at creation
   std::thread worker;
 
   double now() const {
@@ -361,6 +362,8 @@ int pb_srv_create(const pb_srv_config *cfg, pb_srv **out) {
     s->budget = (size_t)(0.9 * (double)fr);
   }
   if (const char *t = std::getenv("PB_SRV_TRACE")) s->trace = t[0] && t[0] != '0';
+  if (cfg->reserve_bytes)  // without the memory free, the server grows the pool as it goes
+    s->reserved = pb_pool_reserve(std::min(cfg->reserve_bytes, s->budget)) == PB_OK;
   s->worker = std::thread(scheduler, s);
   *out = s;
   return PB_OK;
@@ -375,6 +378,7 @@ int pb_srv_destroy(pb_srv *s) {
   s->cv_work.notify_all();
   if (s->worker.joinable()) s->worker.join();
   if (s->batch) pb_batch_destroy(s->batch);
+  if (s->reserved) pb_pool_trim();
   delete s;
   return PB_OK;
 }

@@ -29,7 +29,8 @@ class Server:
     def __init__(self, hbm_budget: float = 0, gaussian: bool = True,
                  fp64_velocities: bool | None = None, fp64_forces: bool = False,
                  chunk_ms: float = 50.0, max_atoms: int = 0, max_jobs: int = 0,
-                 force_threads: int = 256, seg_scale: float = 1.0):
+                 force_threads: int = 256, seg_scale: float = 1.0,
+                 reserve: float | None = None):
         self.lib = L.lib()
         if fp64_velocities is None:
             fp64_velocities = gaussian
@@ -44,6 +45,9 @@ class Server:
         cfg.mode = L.MODE_GAUSS if gaussian else L.MODE_VV
         cfg.force_threads = int(force_threads)
         cfg.seg_scale = float(seg_scale)
+        # device memory taken into the allocator's pool up front (None: the
+        # whole budget, as a serving engine pre-allocates its memory budget)
+        cfg.reserve_bytes = (C.c_size_t(-1).value if reserve is None else int(reserve))
         h = C.c_void_p()
         L.check(self.lib.pb_srv_create(C.byref(cfg), C.byref(h)), "pb_srv_create")
         self.h = h
