@@ -410,10 +410,11 @@ int pb_batch_estimate_bytes(const uint32_t *natoms, const float *cells6, const f
   if (!natoms || !cells6 || !rmax || !bytes || nsys == 0) return PB_ERR_ARG;
   // per atom: r, F[2], rs (16 B each), minv, mass, key, pid_tmp, pid, slot
   // (4 B each), the overflow list entry (8 B), x, y, z, type mirrors of rs
-  // (16 B), type (2 B), velocities (16 or 24 B), sysid (4 B), fixed-point
-  // force sums (48 B)
+  // (16 B), type (2 B), velocities (16 or 24 B), sysid (4 B), and for the
+  // half-shell kernel its fixed-point force sums (48 B)
+  const bool half = (flags & PB_MD_HALF_SHELL) && !(flags & PB_MD_ACC_FP64);
   const size_t per_atom = 16 * 4 + 4 * 6 + 8 + 16 + 2 + ((flags & PB_MD_VEL_FP64) ? 24 : 16) +
-                          (nsys > 1 ? 4 : 0) + 48;
+                          (nsys > 1 ? 4 : 0) + (half ? 48 : 0);
   // per cell: the bucket, sized by the densest system as the engine does
   double apc_max = 0.0;
   for (uint32_t s = 0; s < nsys; ++s) {

@@ -130,6 +130,83 @@ struct Plan {
   std::vector<ForceItem> items;  // system 0, cell0 0
 };
 
+// A plan's tables in device memory (per device, kept for the process): a new
+// batch's items and column tables are expanded from them on the device, so a
+// repack of ~1,500 systems uploads one record per system instead of ~10 MB
+// of items built on the host.
+struct DevPlan {
+  std::shared_ptr<const Plan> keep;  // the host plan stays alive with its key
+  ForceItem *items = nullptr;
+  uint32_t *rank = nullptr, *xy = nullptr;
+};
+
+const DevPlan *device_plan(const std::shared_ptr<const Plan> &p) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const Plan *>, DevPlan> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  const auto key = std::make_pair(dev, p.get());
+  auto it = cache.find(key);
+  if (it != cache.end()) return &it->second;
+  if (cache.size() > 4096) {  // many distinct grids: start over (cudaFree waits for the device)
+    for (auto &kv : cache) {
+      cudaSetDevice(kv.first.first);
+      cudaFree(kv.second.items);
+      cudaFree(kv.second.rank);
+      cudaFree(kv.second.xy);
+    }
+    cudaSetDevice(dev);
+    cache.clear();
+  }
+  DevPlan d;
+  d.keep = p;
+  const size_t ni = std::max<size_t>(1, p->items.size()), nc = std::max<size_t>(1, p->rank.size());
+  bool ok = cudaMalloc(&d.items, sizeof(ForceItem) * ni) == cudaSuccess &&
+            cudaMalloc(&d.rank, 4 * nc) == cudaSuccess && cudaMalloc(&d.xy, 4 * nc) == cudaSuccess;
+  ok = ok &&
+       cudaMemcpy(d.items, p->items.data(), sizeof(ForceItem) * p->items.size(),
+                  cudaMemcpyHostToDevice) == cudaSuccess &&
+       cudaMemcpy(d.rank, p->rank.data(), 4 * p->rank.size(), cudaMemcpyHostToDevice) ==
+           cudaSuccess &&
+       cudaMemcpy(d.xy, p->xy.data(), 4 * p->xy.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+  if (!ok) {
+    cudaFree(d.items);
+    cudaFree(d.rank);
+    cudaFree(d.xy);
+    cudaGetLastError();
+    return nullptr;
+  }
+  return &(cache[key] = std::move(d));
+}
+
+// One system's share of the expansion: its plan's device tables and where its
+// items, columns and cells start in the batch.
+struct SysPlan {
+  const ForceItem *items;
+  const uint32_t *rank, *xy;
+  uint32_t nitems, ncols, item0, col0, cell0;
+};
+
+// Block s writes system s's items (its index, cell keys offset by its first
+// cell) and column tables: the same records the host would build.
+__global__ void k_expand_plans(const SysPlan *sp, ForceItem *items, uint32_t *rank,
+                               uint32_t *xy) {
+  const SysPlan P = sp[blockIdx.x];
+  for (uint32_t k = threadIdx.x; k < P.nitems; k += blockDim.x) {
+    ForceItem it = P.items[k];
+    it.sys = blockIdx.x;
+#pragma unroll
+    for (int c = 0; c < 9; ++c)
+      if (it.kbase[c] != kNoCell) it.kbase[c] += P.cell0;
+    items[P.item0 + k] = it;
+  }
+  for (uint32_t k = threadIdx.x; k < P.ncols; k += blockDim.x) {
+    rank[P.col0 + k] = P.rank[k];
+    xy[P.col0 + k] = P.xy[k];
+  }
+}
+
 std::shared_ptr<const Plan> cached_plan(const Grid &g, int seg) {
   static std::mutex mu;
   static std::map<PlanKey, std::shared_ptr<const Plan>> cache;
@@ -287,8 +364,10 @@ int engine_init(Engine &e, const uint32_t *natoms, uint32_t nsys, uint32_t flags
             dalloc(e, &e.d_sysint, nsys) == cudaSuccess && dalloc(e, &e.d_map, e.nblocks) == cudaSuccess &&
             dalloc(e, &e.ipartials, (size_t)8 * e.nblocks) == cudaSuccess &&
             dalloc(e, &e.sc, nsys) == cudaSuccess && dalloc(e, &e.status, nsys) == cudaSuccess &&
-            dalloc(e, &e.d_fac, nsys) == cudaSuccess && dalloc(e, &e.d_lj, nsys) == cudaSuccess &&
-            dalloc(e, &e.facc, (size_t)6 * N) == cudaSuccess;
+            dalloc(e, &e.d_fac, nsys) == cudaSuccess && dalloc(e, &e.d_lj, nsys) == cudaSuccess;
+  // the half-shell kernel's fixed-point force sums (48 B/atom), only where it runs
+  const bool half = (flags & PB_MD_HALF_SHELL) && !(flags & PB_MD_ACC_FP64);
+  if (half) ok = ok && dalloc(e, &e.facc, (size_t)6 * N) == cudaSuccess;
   if (flags & PB_MD_VEL_FP64)
     ok = ok && dalloc(e, &e.vd, (size_t)3 * N) == cudaSuccess;
   else
@@ -301,7 +380,7 @@ int engine_init(Engine &e, const uint32_t *natoms, uint32_t nsys, uint32_t flags
   if (e.v) E_CUDA(cudaMemsetAsync(e.v, 0, sizeof(float4) * N, e.stream));
   if (e.vd) E_CUDA(cudaMemsetAsync(e.vd, 0, sizeof(double) * 3 * N, e.stream));
   E_CUDA(cudaMemsetAsync(e.type, 0, sizeof(uint16_t) * N, e.stream));
-  E_CUDA(cudaMemsetAsync(e.facc, 0, sizeof(unsigned long long) * 6 * N, e.stream));
+  if (e.facc) E_CUDA(cudaMemsetAsync(e.facc, 0, sizeof(unsigned long long) * 6 * N, e.stream));
   E_CUDA(cudaMemsetAsync(e.sc, 0, sizeof(DevScalars) * nsys, e.stream));
   E_CUDA(cudaMemsetAsync(e.status, 0, sizeof(uint32_t) * nsys, e.stream));
   E_CUDA(cudaMemcpyAsync(e.d_map, map.data(), sizeof(BlockMap) * e.nblocks, cudaMemcpyHostToDevice,
@@ -542,8 +621,6 @@ int engine_setup_cells(Engine &e) {
   e.nl_built = false;  // a list indexes the old sorted slots
   free_cells(e);
   engine_drop_graph(e);
-  std::vector<uint32_t> rank_all, xy_all;
-  std::vector<ForceItem> items;
   std::vector<SysDesc> sd(e.nsys);
   e.item0.assign(e.nsys + 1, 0);
   e.cell0.assign(e.nsys + 1, 0);
@@ -552,9 +629,8 @@ int engine_setup_cells(Engine &e) {
   e.cap_max = 0;
   e.cap_half_max = 0;
   double apc_max = 0.0;
-  // grids and plans first, so that the item and column arrays are sized once
+  // grids and plans first, then each system's place in the batch
   std::vector<std::shared_ptr<const Plan>> plans(e.nsys);
-  size_t nitem_all = 0, ncol_all = 0;
   for (uint32_t s = 0; s < e.nsys; ++s) {
     SysParams &P = e.sp[s];
     if (!P.cell_set) return fail(e, PB_ERR_STATE, "set the cell first");
@@ -574,25 +650,26 @@ int engine_setup_cells(Engine &e) {
     e.cap_max = std::max(e.cap_max, P.cap);
     e.cap_half_max = std::max(e.cap_half_max, P.cap_half);
     plans[s] = cached_plan(g, P.seg);
-    nitem_all += plans[s]->items.size();
-    ncol_all += plans[s]->rank.size();
   }
-  items.reserve(nitem_all);
-  rank_all.reserve(ncol_all);
-  xy_all.reserve(ncol_all);
+  std::vector<SysPlan> spl(e.nsys);
+  uint64_t nitems = 0, ncols = 0;
   for (uint32_t s = 0; s < e.nsys; ++s) {
     SysParams &P = e.sp[s];
     const Grid g = P.grid;
     const Plan &plan = *plans[s];
-    const std::vector<uint32_t> &rank = plan.rank, &xy = plan.xy;
+    const DevPlan *dp = device_plan(plans[s]);
+    if (!dp) return fail(e, PB_ERR_OOM, "work item tables");
+    const std::vector<uint32_t> &rank = plan.rank;
     e.cell0[s] = (uint32_t)ncells;
-    e.item0[s] = (uint32_t)items.size();
-    for (ForceItem it : plan.items) {  // the system's items: its index and first cell key
-      it.sys = s;
-      for (auto &k : it.kbase)
-        if (k != kNoCell) k += (uint32_t)ncells;
-      items.push_back(it);
-    }
+    e.item0[s] = (uint32_t)nitems;
+    spl[s] = SysPlan{dp->items,
+                     dp->rank,
+                     dp->xy,
+                     (uint32_t)plan.items.size(),
+                     (uint32_t)rank.size(),
+                     (uint32_t)nitems,
+                     (uint32_t)ncols,
+                     (uint32_t)ncells};
     P.key_of_ref.clear();
     P.ref_of_key.clear();
     if (e.nsys == 1) {  // reference cell id <-> key, for the single-system getters
@@ -612,7 +689,7 @@ int engine_setup_cells(Engine &e) {
     D.atom0 = e.atom0[s];
     D.natoms = P.n;
     D.cell0 = (uint32_t)ncells;
-    D.col0 = (uint32_t)rank_all.size();
+    D.col0 = (uint32_t)ncols;
     D.vd0 = 3 * e.atom0[s];
     D.lj = s;
     D.dt = P.dt;
@@ -620,15 +697,16 @@ int engine_setup_cells(Engine &e) {
     D.cap_half = P.cap_half;
     D.mirror0 = mirror;
     mirror += (P.n + 3u) & ~3u;
-    rank_all.insert(rank_all.end(), rank.begin(), rank.end());
-    xy_all.insert(xy_all.end(), xy.begin(), xy.end());
+    nitems += plan.items.size();
+    ncols += rank.size();
     ncells += g.ncells;
-    if (ncells >= 0xffffffffull) return fail(e, PB_ERR_ARG, "too many cells");
+    if (ncells >= 0xffffffffull || nitems >= 0xffffffffull)
+      return fail(e, PB_ERR_ARG, "too many cells");
   }
-  e.item0[e.nsys] = (uint32_t)items.size();
+  e.item0[e.nsys] = (uint32_t)nitems;
   e.cell0[e.nsys] = (uint32_t)ncells;
   e.ncells = (uint32_t)ncells;
-  e.nitems = (uint32_t)items.size();
+  e.nitems = (uint32_t)nitems;
   e.mirrorN = mirror + 4u;
   const uint32_t N = e.N, C = e.ncells;
   e.bucket_cap = (uint32_t)choose_bucket_cap(apc_max);
@@ -645,11 +723,11 @@ int engine_setup_cells(Engine &e) {
             dalloc(e, &e.pid, N) == cudaSuccess && dalloc(e, &e.slot, N) == cudaSuccess &&
             dalloc(e, &e.rs, N) == cudaSuccess && dalloc(e, &e.xs, e.mirrorN) == cudaSuccess &&
             dalloc(e, &e.ys, e.mirrorN) == cudaSuccess && dalloc(e, &e.zs, e.mirrorN) == cudaSuccess &&
-            dalloc(e, &e.ts, e.mirrorN) == cudaSuccess && dalloc(e, &e.colrank, rank_all.size()) == cudaSuccess &&
-            dalloc(e, &e.colxy, xy_all.size()) == cudaSuccess &&
-            dalloc(e, &e.d_sys, e.nsys) == cudaSuccess && dalloc(e, &e.d_items, items.size()) == cudaSuccess &&
+            dalloc(e, &e.ts, e.mirrorN) == cudaSuccess && dalloc(e, &e.colrank, ncols) == cudaSuccess &&
+            dalloc(e, &e.colxy, ncols) == cudaSuccess &&
+            dalloc(e, &e.d_sys, e.nsys) == cudaSuccess && dalloc(e, &e.d_items, nitems) == cudaSuccess &&
             dalloc(e, &e.d_item0, e.nsys + 1) == cudaSuccess &&
-            dalloc(e, &e.fpartials, (size_t)4 * items.size()) == cudaSuccess &&
+            dalloc(e, &e.fpartials, (size_t)4 * nitems) == cudaSuccess &&
             dalloc(e, &e.fqueue, 2) == cudaSuccess;
   if (!ok) {
     free_cells(e);
@@ -659,14 +737,15 @@ int engine_setup_cells(Engine &e) {
   E_CUDA(cudaMemsetAsync(e.tcount, 0, sizeof(uint32_t) * e.ntile, e.stream));
   E_CUDA(cudaMemsetAsync(e.cctl, 0, sizeof(uint32_t) * 2, e.stream));
   E_CUDA(cudaMemsetAsync(e.fqueue, 0, sizeof(uint32_t) * 2, e.stream));
-  E_CUDA(cudaMemcpyAsync(e.colrank, rank_all.data(), 4 * rank_all.size(), cudaMemcpyHostToDevice,
+  SysPlan *d_spl = nullptr;
+  E_CUDA(engine_alloc_bytes(e, (void **)&d_spl, sizeof(SysPlan) * e.nsys));
+  E_CUDA(cudaMemcpyAsync(d_spl, spl.data(), sizeof(SysPlan) * e.nsys, cudaMemcpyHostToDevice,
                          e.stream));
-  E_CUDA(cudaMemcpyAsync(e.colxy, xy_all.data(), 4 * xy_all.size(), cudaMemcpyHostToDevice,
-                         e.stream));
+  k_expand_plans<<<e.nsys, 256, 0, e.stream>>>(d_spl, e.d_items, e.colrank, e.colxy);
+  E_CUDA(cudaGetLastError());
+  engine_free_bytes(e, d_spl);
   E_CUDA(cudaMemcpyAsync(e.d_sys, sd.data(), sizeof(SysDesc) * e.nsys, cudaMemcpyHostToDevice,
                          e.stream));
-  E_CUDA(cudaMemcpyAsync(e.d_items, items.data(), sizeof(ForceItem) * items.size(),
-                         cudaMemcpyHostToDevice, e.stream));
   E_CUDA(cudaMemcpyAsync(e.d_item0, e.item0.data(), 4 * (size_t)(e.nsys + 1),
                          cudaMemcpyHostToDevice, e.stream));
   E_CUDA(cudaStreamSynchronize(e.stream));
@@ -764,7 +843,7 @@ ForceBufs engine_fbufs(Engine &e) {
   b.status = e.status;
   b.steps_left = e.steps_left;
   b.facc = e.facc;
-  b.fbig = e.facc + (size_t)3 * e.N;
+  b.fbig = e.facc ? e.facc + (size_t)3 * e.N : nullptr;
   b.nacc = e.N;
   b.cap_half = (int)e.cap_half_max;
   b.map = e.d_map;
