@@ -100,7 +100,7 @@ int pb_batch_repack(const pb_batch *old, const int32_t *src, const uint32_t *nat
   }
   pb_batch *b = new pb_batch;
   Engine &e = b->e;
-  int rc = engine_init(e, n.data(), nsys, o.flags);
+  int rc = engine_init(e, n.data(), nsys, o.flags, false);  // the gather below writes the state
   if (rc) {
     engine_free(e);
     delete b;

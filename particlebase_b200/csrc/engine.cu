@@ -317,7 +317,8 @@ void engine_drop_graph(Engine &e) {
   e.graph_dt.clear();
 }
 
-int engine_init(Engine &e, const uint32_t *natoms, uint32_t nsys, uint32_t flags) {
+int engine_init(Engine &e, const uint32_t *natoms, uint32_t nsys, uint32_t flags,
+                bool zero_state) {
   if (!natoms || nsys == 0) return fail(e, PB_ERR_ARG, "no systems");
   e.flags = flags;
   e.nsys = nsys;
@@ -374,12 +375,14 @@ int engine_init(Engine &e, const uint32_t *natoms, uint32_t nsys, uint32_t flags
     ok = ok && dalloc(e, &e.v, N) == cudaSuccess;
   if (nsys > 1) ok = ok && dalloc(e, &e.sysid, N) == cudaSuccess;
   if (!ok) return fail(e, PB_ERR_OOM, "device allocation failed");
-  E_CUDA(cudaMemsetAsync(e.r, 0, sizeof(float4) * N, e.stream));
-  E_CUDA(cudaMemsetAsync(e.F[0], 0, sizeof(float4) * N, e.stream));
-  E_CUDA(cudaMemsetAsync(e.F[1], 0, sizeof(float4) * N, e.stream));
-  if (e.v) E_CUDA(cudaMemsetAsync(e.v, 0, sizeof(float4) * N, e.stream));
-  if (e.vd) E_CUDA(cudaMemsetAsync(e.vd, 0, sizeof(double) * 3 * N, e.stream));
-  E_CUDA(cudaMemsetAsync(e.type, 0, sizeof(uint16_t) * N, e.stream));
+  if (zero_state) {
+    E_CUDA(cudaMemsetAsync(e.r, 0, sizeof(float4) * N, e.stream));
+    E_CUDA(cudaMemsetAsync(e.F[0], 0, sizeof(float4) * N, e.stream));
+    E_CUDA(cudaMemsetAsync(e.F[1], 0, sizeof(float4) * N, e.stream));
+    if (e.v) E_CUDA(cudaMemsetAsync(e.v, 0, sizeof(float4) * N, e.stream));
+    if (e.vd) E_CUDA(cudaMemsetAsync(e.vd, 0, sizeof(double) * 3 * N, e.stream));
+    E_CUDA(cudaMemsetAsync(e.type, 0, sizeof(uint16_t) * N, e.stream));
+  }
   if (e.facc) E_CUDA(cudaMemsetAsync(e.facc, 0, sizeof(unsigned long long) * 6 * N, e.stream));
   E_CUDA(cudaMemsetAsync(e.sc, 0, sizeof(DevScalars) * nsys, e.stream));
   E_CUDA(cudaMemsetAsync(e.status, 0, sizeof(uint32_t) * nsys, e.stream));

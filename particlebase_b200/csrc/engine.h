@@ -123,7 +123,10 @@ struct Engine {
 };
 
 // All return pb_status codes; on failure e.err says why.
-int engine_init(Engine &e, const uint32_t *natoms, uint32_t nsys, uint32_t flags);
+// zero_state = false leaves r, v, F and type unwritten: a repack's gather
+// writes every atom of them (continuing systems copied, new ones zeroed).
+int engine_init(Engine &e, const uint32_t *natoms, uint32_t nsys, uint32_t flags,
+                bool zero_state = true);
 void engine_free(Engine &e);
 int engine_set_stream(Engine &e, cudaStream_t s);
 int engine_upload_lj(Engine &e);

@@ -502,7 +502,25 @@ __global__ void __launch_bounds__(kIntThreads) k_fill_sysid(const BlockMap *map,
 __global__ void __launch_bounds__(kIntThreads) k_gather_state(GatherArgs g) {
   const BlockMap m = g.map[blockIdx.x];
   const GatherSrc q = g.gs[m.sys];
-  if (q.src < 0) return;
+  if (q.src < 0) {  // a new system starts from zeros, as a new engine's arrays do
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
+      const uint32_t off = m.k * kIntAtoms + t, i = m.i0 + t;
+      g.r[i] = z4;
+      g.F0[i] = z4;
+      g.F1[i] = z4;
+      g.type[i] = 0;
+      if (g.v) g.v[i] = z4;
+      if (g.vd) {
+        const SysInt &S = g.sys[m.sys];
+        const size_t n = S.natoms, dst = (size_t)S.vd0 + off;
+        g.vd[dst] = 0.0;
+        g.vd[dst + n] = 0.0;
+        g.vd[dst + 2 * n] = 0.0;
+      }
+    }
+    return;
+  }
   for (uint32_t t = threadIdx.x; t < m.n; t += kIntThreads) {
     const uint32_t off = m.k * kIntAtoms + t;  // atom within its system
     const uint32_t i = m.i0 + t, o = q.o_atom0 + off;

@@ -93,7 +93,7 @@ cudaError_t launch_fill_sysid(const BlockMap *map, uint32_t nblocks, uint32_t *s
 
 // State of one system of a new batch that continues a system of an old one.
 struct GatherSrc {
-  int32_t src;       // old system, or -1 for a new system (left untouched)
+  int32_t src;       // old system, or -1 for a new system (zeroed)
   uint32_t o_atom0;  // its first atom in the old arrays
   uint8_t fb0, fb1;  // old force buffer that feeds new F[0] and new F[1]
 };
@@ -112,7 +112,7 @@ struct GatherArgs {
   float *minv, *mass;
   uint16_t *type;
 };
-// Copy every continuing system's per-atom state in one launch.
+// Copy every continuing system's per-atom state, and zero every new system's, in one launch.
 cudaError_t launch_gather_state(const GatherArgs &g, cudaStream_t s);
 
 // Host helpers: integration blocks of kIntAtoms atoms aligned to each
