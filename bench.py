@@ -596,7 +596,7 @@ def main(argv=None) -> int:
                          "c5 under 'kob_andersen'")
     ap.add_argument("--jobs", type=int, default=2000,
                     help="served jobs of the C4 stream (default: all 2,000)")
-    ap.add_argument("--chunk-ms", type=float, default=50.0)
+    ap.add_argument("--chunk-ms", type=float, default=100.0)
     ap.add_argument("--ka-atoms", type=int, default=8_388_608)
     ap.add_argument("--ka-steps", type=int, default=300)
     ap.add_argument("--replicas", type=int, default=256)

@@ -399,7 +399,7 @@ typedef struct pb_srv_config {
   size_t hbm_budget;      /* bytes the resident batch may hold (estimate); 0 = 90% of free */
   uint64_t max_atoms;     /* resident atom cap (0 = none): bounds the step time */
   uint32_t max_jobs;      /* resident job cap (0 = none) */
-  float chunk_ms;         /* target GPU time between chunk boundaries (0 = 50 ms) */
+  float chunk_ms;         /* target GPU time between chunk boundaries (0 = 100 ms) */
   uint32_t flags;         /* PB_MD_VEL_FP64 | PB_MD_ACC_FP64 */
   int mode;               /* PB_MODE_VV or PB_MODE_GAUSS */
   int force_threads;      /* 0 = default (256) */

@@ -309,7 +309,7 @@ void scheduler(pb_srv *s) {
     // a chunk lasts at least four repacks, so repacking costs at most a fifth
     // of the GPU time even when jobs arrive and leave at every boundary
     const double chunk_ms =
-        std::max(s->cfg.chunk_ms > 0 ? (double)s->cfg.chunk_ms : 50.0, 4.0 * s->last_repack_ms);
+        std::max(s->cfg.chunk_ms > 0 ? (double)s->cfg.chunk_ms : 100.0, 4.0 * s->last_repack_ms);
     double want = chunk_ms / std::max(1e-6, s->ms_per_atom_step * (double)atoms);
     uint32_t K = (uint32_t)std::max(2.0, std::min(want, 1e6));
     K += K & 1u;

@@ -28,7 +28,7 @@ STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
 class Server:
     def __init__(self, hbm_budget: float = 0, gaussian: bool = True,
                  fp64_velocities: bool | None = None, fp64_forces: bool = False,
-                 chunk_ms: float = 50.0, max_atoms: int = 0, max_jobs: int = 0,
+                 chunk_ms: float = 100.0, max_atoms: int = 0, max_jobs: int = 0,
                  force_threads: int = 256, seg_scale: float = 1.0,
                  reserve: float | None = None):
         self.lib = L.lib()
