@@ -78,3 +78,29 @@ def test_budget_limits_the_resident_set(cuda_lib):
         srv.submit(big.system(), 10, DT)
     assert e.value.code == 6  # PB_ERR_OOM
     srv.close()
+
+
+def test_pool_reserve_and_trim(cuda_lib):
+    """pb_pool_reserve takes device memory into the library's pool at once (a
+    server does it at creation so that repacks never wait for the pool to
+    grow); pb_pool_trim hands the unused part back."""
+    import torch
+    from particlebase_b200 import _lib as L
+    from particlebase_b200.md import from_system
+    lib = L.lib()
+    assert lib.pb_pool_trim() == 0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    gb = 1 << 30
+    assert lib.pb_pool_reserve(2 * gb) == 0
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free0 - free1 >= 2 * gb - (64 << 20)
+    p = from_system(W.config_c1(), gaussian=True)  # a handle allocates from the reservation
+    p.run(DT, 2)
+    assert p.status() == 0
+    p.close()
+    assert lib.pb_pool_trim() == 0
+    assert torch.cuda.mem_get_info()[0] >= free0 - (64 << 20)
+    # more than the device holds: refused
+    total = torch.cuda.mem_get_info()[1]
+    assert lib.pb_pool_reserve(total + gb) == 6  # PB_ERR_OOM
