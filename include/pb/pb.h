@@ -405,10 +405,11 @@ typedef struct pb_srv_config {
   int force_threads;      /* 0 = default (256) */
   float seg_scale;        /* 0 = 1.0 */
   size_t reserve_bytes;   /* device memory taken into the library's pool at creation
-                             (pb_pool_reserve) and handed back by pb_srv_destroy, so
-                             that repacks never wait for the pool to grow; 0 = none,
-                             SIZE_MAX = the whole HBM budget.  Not available: the
-                             server runs without it. */
+                             (pb_pool_reserve), so that repacks never wait for the pool
+                             to grow; pb_srv_destroy then trims the pool (pb_pool_trim),
+                             which hands back the unused memory of every handle.
+                             0 = none, SIZE_MAX = the whole HBM budget.  Not available:
+                             the server runs without it. */
 } pb_srv_config;
 
 typedef struct pb_srv_job {

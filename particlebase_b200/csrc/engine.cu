@@ -99,10 +99,14 @@ int engine_pool_reserve(size_t bytes) {
   if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return PB_ERR_CUDA;
   void *p = nullptr;
   int rc = PB_OK;
+  uint64_t held = 0;
+  cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &held);
   if (cudaMallocFromPoolAsync(&p, bytes, pool, s) == cudaSuccess) {
     cudaFreeAsync(p, s);
   } else {
     cudaGetLastError();  // allocation failures are not sticky
+    // a failed growth can leave the pages it did map in the pool: give them back
+    cudaMemPoolTrimTo(pool, (size_t)held);
     rc = PB_ERR_OOM;
   }
   if (cudaStreamSynchronize(s) != cudaSuccess) rc = PB_ERR_CUDA;
@@ -136,48 +140,53 @@ struct Plan {
 // of items built on the host.
 struct DevPlan {
   std::shared_ptr<const Plan> keep;  // the host plan stays alive with its key
+  int dev = 0;
   ForceItem *items = nullptr;
   uint32_t *rank = nullptr, *xy = nullptr;
+  DevPlan() = default;
+  DevPlan(const DevPlan &) = delete;
+  DevPlan &operator=(const DevPlan &) = delete;
+  ~DevPlan() {  // the last user is done with it (cudaFree waits for the device)
+    int cur = 0;
+    if (cudaGetDevice(&cur) != cudaSuccess) return;
+    cudaSetDevice(dev);
+    cudaFree(items);
+    cudaFree(rank);
+    cudaFree(xy);
+    cudaSetDevice(cur);
+  }
 };
 
-const DevPlan *device_plan(const std::shared_ptr<const Plan> &p) {
+// The cache holds one reference and every engine set-up that uses a plan
+// another, so a cache that starts over frees no table still being expanded.
+std::shared_ptr<const DevPlan> device_plan(const std::shared_ptr<const Plan> &p) {
   static std::mutex mu;
-  static std::map<std::pair<int, const Plan *>, DevPlan> cache;
+  static std::map<std::pair<int, const Plan *>, std::shared_ptr<const DevPlan>> cache;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
   std::lock_guard<std::mutex> lk(mu);
   const auto key = std::make_pair(dev, p.get());
   auto it = cache.find(key);
-  if (it != cache.end()) return &it->second;
-  if (cache.size() > 4096) {  // many distinct grids: start over (cudaFree waits for the device)
-    for (auto &kv : cache) {
-      cudaSetDevice(kv.first.first);
-      cudaFree(kv.second.items);
-      cudaFree(kv.second.rank);
-      cudaFree(kv.second.xy);
-    }
-    cudaSetDevice(dev);
-    cache.clear();
-  }
-  DevPlan d;
-  d.keep = p;
+  if (it != cache.end()) return it->second;
+  if (cache.size() > 4096) cache.clear();  // many distinct grids: start over
+  auto d = std::make_shared<DevPlan>();
+  d->keep = p;
+  d->dev = dev;
   const size_t ni = std::max<size_t>(1, p->items.size()), nc = std::max<size_t>(1, p->rank.size());
-  bool ok = cudaMalloc(&d.items, sizeof(ForceItem) * ni) == cudaSuccess &&
-            cudaMalloc(&d.rank, 4 * nc) == cudaSuccess && cudaMalloc(&d.xy, 4 * nc) == cudaSuccess;
+  bool ok = cudaMalloc(&d->items, sizeof(ForceItem) * ni) == cudaSuccess &&
+            cudaMalloc(&d->rank, 4 * nc) == cudaSuccess && cudaMalloc(&d->xy, 4 * nc) == cudaSuccess;
   ok = ok &&
-       cudaMemcpy(d.items, p->items.data(), sizeof(ForceItem) * p->items.size(),
+       cudaMemcpy(d->items, p->items.data(), sizeof(ForceItem) * p->items.size(),
                   cudaMemcpyHostToDevice) == cudaSuccess &&
-       cudaMemcpy(d.rank, p->rank.data(), 4 * p->rank.size(), cudaMemcpyHostToDevice) ==
+       cudaMemcpy(d->rank, p->rank.data(), 4 * p->rank.size(), cudaMemcpyHostToDevice) ==
            cudaSuccess &&
-       cudaMemcpy(d.xy, p->xy.data(), 4 * p->xy.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+       cudaMemcpy(d->xy, p->xy.data(), 4 * p->xy.size(), cudaMemcpyHostToDevice) == cudaSuccess;
   if (!ok) {
-    cudaFree(d.items);
-    cudaFree(d.rank);
-    cudaFree(d.xy);
-    cudaGetLastError();
-    return nullptr;
+    cudaGetLastError();  // allocation failures are not sticky
+    return nullptr;      // d frees what it holds
   }
-  return &(cache[key] = std::move(d));
+  cache[key] = d;
+  return d;
 }
 
 // One system's share of the expansion: its plan's device tables and where its
@@ -655,12 +664,14 @@ int engine_setup_cells(Engine &e) {
     plans[s] = cached_plan(g, P.seg);
   }
   std::vector<SysPlan> spl(e.nsys);
+  std::vector<std::shared_ptr<const DevPlan>> dplans(e.nsys);  // held until the expansion is done
   uint64_t nitems = 0, ncols = 0;
   for (uint32_t s = 0; s < e.nsys; ++s) {
     SysParams &P = e.sp[s];
     const Grid g = P.grid;
     const Plan &plan = *plans[s];
-    const DevPlan *dp = device_plan(plans[s]);
+    dplans[s] = device_plan(plans[s]);
+    const DevPlan *dp = dplans[s].get();
     if (!dp) return fail(e, PB_ERR_OOM, "work item tables");
     const std::vector<uint32_t> &rank = plan.rank;
     e.cell0[s] = (uint32_t)ncells;

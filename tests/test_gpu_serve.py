@@ -101,6 +101,7 @@ def test_pool_reserve_and_trim(cuda_lib):
     p.close()
     assert lib.pb_pool_trim() == 0
     assert torch.cuda.mem_get_info()[0] >= free0 - (64 << 20)
-    # more than the device holds: refused
+    # more than the device holds: refused, and nothing is kept
     total = torch.cuda.mem_get_info()[1]
     assert lib.pb_pool_reserve(total + gb) == 6  # PB_ERR_OOM
+    assert torch.cuda.mem_get_info()[0] >= free0 - (64 << 20)
