@@ -291,28 +291,34 @@ def run_ours(args, dist: Dist) -> dict:
     traffic = profiled_traffic("k_force")
 
     grid = [int(x) for x in p.grid()[0]]
+    build_kernels = p.cell_build_kernels()
     # the device-timed handle is done: the end-to-end leg runs alone, as a
     # driver with one handle would (its memory returns to the pool)
     p.close()
 
     # e2e through the public API with host buffers (reference driver loop),
-    # over the workload's 500 steps (set-up and import included)
+    # over the workload's 500 steps (set-up and import included).  The 500
+    # host round trips are sensitive to load on the host, so the leg runs
+    # three times from scratch and the median time is the value.
     e2e_steps = C2_STEPS
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    q = from_system(s, gaussian=True, fp64_velocities=False, half_shell=half)
-    q.clearForce()
-    temps = []
-    for _ in range(e2e_steps):
-        q.run(DT, 1)
-        temps.append(q.calcTemp())
-    r_final = q.getPosition()
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
+    e2e_times = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        q = from_system(s, gaussian=True, fp64_velocities=False, half_shell=half)
+        q.clearForce()
+        temps = []
+        for _ in range(e2e_steps):
+            q.run(DT, 1)
+            temps.append(q.calcTemp())
+        r_final = q.getPosition()
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+        q.close()
+    e2e_s = sorted(e2e_times)[1]
     e2e_value = replica_rate(dist.ws, s.n, e2e_steps, dist.reduce(e2e_s, "max"))
     h2d = s.n * (16 + 16 + 4 + 4 + 2)
     d2h = 8 * e2e_steps + r_final.nbytes
-    q.close()
 
     nlist = neighbor_list_leg(s, dist) if dist.rank == 0 else None
 
@@ -345,13 +351,14 @@ def run_ours(args, dist: Dist) -> dict:
                        if hbm else None}},
         "clocks": clocks,
         "device_status": status,
-        # per step: 6 cell-build kernels, the force kernel (+ the fixed-point
-        # finish with the half shell), the two Gaussian passes
-        "gpu_launches": (6 + (2 if half else 1) + 2) * steps,
+        # per step: the cell build's kernels (2 or 6), the force kernel (+ the
+        # fixed-point finish with the half shell), the two Gaussian passes
+        "gpu_launches": (build_kernels + (2 if half else 1) + 2) * steps,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
                 "d2h_bytes_per_step": d2h / e2e_steps, "steps": e2e_steps,
                 "includes": "import from host, per-step pb_md_run + temperature read-back, "
-                            "final positions to host"},
+                            "final positions to host",
+                "passes_s": [round(t, 4) for t in e2e_times], "reported": "median of 3 passes"},
     }
     if nlist is not None:
         out["neighbor_list"] = nlist

@@ -215,6 +215,10 @@ int pb_md_profile(pb_md *h, float dt, int mode, uint32_t steps, double ms[3]);
  * over the 27-cell stencil (i != j), out[1] = ordered pairs inside the cutoff
  * counted by the last pb_md_force with PB_FORCE_ENERGY. */
 int pb_md_pair_stats(pb_md *h, double out[2]);
+/* Kernels one cell build launches: 2 for the bucket build, 6 for the counting
+ * sort (the engine picks the faster at pb_md_setup_cells; PB_CELL_BUILD fixes
+ * it).  No counterpart in the reference. */
+int pb_md_cell_build_kernels(pb_md *h, uint32_t *kernels);
 
 /* ---- reductions and velocity control -------------------------------------- */
 

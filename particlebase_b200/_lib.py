@@ -126,6 +126,7 @@ def _declare(L: C.CDLL) -> None:
         "pb_md_size": [vp, C.POINTER(u32)],
         "pb_md_profile": [vp, f32, i32, u32, C.POINTER(f64)],
         "pb_md_pair_stats": [vp, C.POINTER(f64)],
+        "pb_md_cell_build_kernels": [vp, C.POINTER(u32)],
         "pb_peak_fp32": [C.POINTER(f64)],
         "pb_cells_build_noalloc": [vp, vp, u32, C.POINTER(f32), f32, vp, vp, vp, vp, vp],
         "pb_cells_build_noalloc_limits": [C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_size_t)],

@@ -263,6 +263,13 @@ int pb_md_profile(pb_md *h, float dt, int mode, uint32_t steps, double ms[3]) {
   return engine_profile(h->e, mode, steps, ms);
 }
 
+int pb_md_cell_build_kernels(pb_md *h, uint32_t *kernels) {
+  if (!h || !kernels) return PB_ERR_ARG;
+  if (!h->e.cells_ready) return fail(h, PB_ERR_STATE, "setup_cells first");
+  *kernels = h->e.cells_bucket ? 2u : 6u;
+  return PB_OK;
+}
+
 int pb_md_pair_stats(pb_md *h, double out[2]) {
   if (!h || !out || !h->e.cells_ready) return PB_ERR_STATE;
   Engine &e = h->e;

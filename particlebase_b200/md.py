@@ -222,6 +222,12 @@ class MDSystem:
         self._ck(self.lib.pb_md_minimize(self.h, int(iters), C.c_float(alpha),
                                          C.c_float(max_disp)), "minimize")
 
+    def cell_build_kernels(self) -> int:
+        """Kernels one cell build launches (2: bucket build, 6: counting sort)."""
+        k = C.c_uint32()
+        self._ck(self.lib.pb_md_cell_build_kernels(self.h, C.byref(k)), "cell_build_kernels")
+        return int(k.value)
+
     def pair_stats(self) -> dict:
         out = (C.c_double * 2)()
         self._ck(self.lib.pb_md_pair_stats(self.h, out), "pair_stats")
